@@ -1,0 +1,343 @@
+"""Benchmark: batched RNS NTT round trip + polymul on B200.
+
+Workload (the batched configuration of the lattice-arithmetic path):
+N = 2^16, L = 24 primes (descending below 2^50, q = 1 mod 2^17), 64
+ciphertexts x 2 polynomials = 128 DCRT polys with uniform residues from a seed,
+one 24-limb plaintext (uniform, kept in the NTT domain in HBM).  One step =
+forward NTT, pointwise product with the plaintext, inverse NTT of all 128
+polys -- one fused cluster launch (`pg_dcrt_polymul_ntt_plain`).  The metric
+counts "2^16 x 24-prime NTTs" (one forward or inverse transform of one 24-limb
+poly): 256 per step.  Inputs are 1.61 GB, larger than the 126 MB L2, so no L2
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  `--impl reference` times the CPU restatement of the
+reference's own algorithm (the oracle port; the Rust reference cannot be built
+here) on the host's cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOG_N, L, POLYS = 16, 24, 128
+N = 1 << LOG_N
+SEED = 0x5EED0001
+NTT_PER_STEP = 2 * POLYS
+METRIC = "2^16x24-prime NTT/s (batched fwd -> x plain -> inv, bit-exact)"
+UNIT = "NTT/s"
+WORKLOAD = {
+    "workload": "batched RNS NTT round trip + polymul: N=2^16, L=24 primes < 2^50 (q = 1 mod 2^17), "
+                "64 ciphertexts x 2 polys, NTT-domain plaintext resident",
+    "N": N, "L": L, "polys": POLYS,
+    "l2": "inputs 1.61 GB per step > 126 MB L2 (no flush needed)",
+}
+# algorithmic bytes of one step: read + write every residue once, read the plaintext once
+ALGO_BYTES = 2 * POLYS * L * N * 8 + L * N * 8
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("polymul_round_trip_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    """One process per GPU under torchrun; returns (rank, world, local_rank, dist-or-None)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        return rank, world, local, dist
+    return rank, world, local, None
+
+
+def dist_max(dist, value: float, local: int) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_reference(moduli, seconds_target=12.0, threads=None):
+    """Time the oracle port of the reference's path (UintNttTable + DcrtPolynomial::mul_assign)
+    on the host cores over a bounded sample of the workload; returns (NTT/s, sample text, threads)."""
+    import oracle as O
+    threads = threads or cpu_threads()
+    ref = O.DcrtTable(LOG_N, moduli)
+    plain = O.uniform_rns(SEED + 7, 0, moduli, N)
+    plain = ref.forward(plain)
+    one = O.uniform_rns(SEED, 0, moduli, N)
+    t0 = time.perf_counter()
+    ref.polymul_roundtrip(one, plain, threads=threads)
+    t1 = time.perf_counter()
+    per_poly = max(t1 - t0, 1e-4)
+    # at least one poly per thread so every core works; bounded to ~seconds_target
+    polys = int(max(threads, min(POLYS, seconds_target / per_poly * threads / max(threads, 1))))
+    polys = max(1, min(POLYS, polys))
+    x = np.concatenate([O.uniform_rns(SEED, p * L, moduli, N) for p in range(polys)])
+    t0 = time.perf_counter()
+    ref.polymul_roundtrip(x, plain, threads=threads)
+    dt = time.perf_counter() - t0
+    return 2 * polys / dt, f"{polys} of {POLYS} polys (24 limbs, N=2^16) round trip, {dt:.2f} s", threads
+
+
+def run_reference(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    import oracle as O
+    moduli = O.ntt_primes(1 << 50, 2 * N, L)
+    vals = []
+    sample = ""
+    thr = cpu_threads()
+    for _ in range(args.warmup):
+        cpu_reference(moduli, seconds_target=2.0, threads=thr)
+    for _ in range(max(1, args.steps)):
+        v, sample, thr = cpu_reference(moduli, seconds_target=max(2.0, 60.0 / max(1, args.steps)), threads=thr)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": NTT_PER_STEP / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded uniform residues)", "config": WORKLOAD,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": "C restatement of UintNttTable/DcrtPolynomial (oracle), OpenMP over rows; " + sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    import primus_b200 as P
+    from primus_b200 import _native as nat
+    nat.call("pg_set_device", local)
+    moduli = P.ntt_primes(1 << 50, 2 * N, L)
+    tab = P.DcrtTable(LOG_N, moduli)
+    stream = P.Stream()
+    data = P.DeviceBuffer(POLYS * L * N)
+    plain = P.DeviceBuffer(L * N)
+    plain_q = P.DeviceBuffer(L * N)
+    tab.fill_uniform(data, POLYS, seed=SEED + rank, stream=stream)
+    tab.fill_uniform(plain, 1, seed=SEED + 7, stream=stream)
+    tab.forward(plain, 1, stream=stream)
+    tab.shoup_prepare(plain, plain_q, 1, stream=stream)
+    stream.synchronize()
+
+    def step():
+        tab.polymul_ntt_plain(data, plain, plain_q, POLYS, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = P.Event(), P.Event()
+    dist_barrier(dist)
+    stream.synchronize()
+    launches0 = P.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    stream.synchronize()
+    launches = P.launch_count() - launches0
+    ms = e0.elapsed_ms(e1)
+    dist_barrier(dist)
+    clocks = sampler.stop()
+    ms_max = dist_max(dist, ms, local)
+    per_step = ms_max / args.steps
+    value = NTT_PER_STEP * world / (per_step / 1e3)
+
+    # ---- plain one-call-per-op GPU form (fwd, mul, inv as separate launches), same data
+    for _ in range(2):
+        tab.forward(data, POLYS, stream=stream)
+        tab.mul(data, plain, POLYS, rhs_polys=1, stream=stream)
+        tab.inverse(data, POLYS, stream=stream)
+    e0.record(stream)
+    plain_steps = max(3, args.steps // 2)
+    for _ in range(plain_steps):
+        tab.forward(data, POLYS, stream=stream)
+        tab.mul(data, plain, POLYS, rhs_polys=1, stream=stream)
+        tab.inverse(data, POLYS, stream=stream)
+    e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_ms(e1) / plain_steps
+
+    # ---- end to end through the public C ABI with pinned host buffers
+    import ctypes as C
+    nbytes = POLYS * L * N * 8
+    hp = C.c_void_p()
+    nat.call("pg_host_alloc", C.byref(hp), nbytes)
+    host = np.ctypeslib.as_array((C.c_uint64 * (POLYS * L * N)).from_address(hp.value))
+    host[:] = data.numpy()
+    for _ in range(2):
+        nat.call("pg_memcpy_h2d", data.ptr, hp.value, nbytes, stream.h)
+        step()
+        nat.call("pg_memcpy_d2h", hp.value, data.ptr, nbytes, stream.h)
+    stream.synchronize()
+    e2e_steps = max(3, min(args.steps, 10))
+    dist_barrier(dist)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        nat.call("pg_memcpy_h2d", data.ptr, hp.value, nbytes, stream.h)
+        step()
+        nat.call("pg_memcpy_d2h", hp.value, data.ptr, nbytes, stream.h)
+    e1.record(stream)
+    stream.synchronize()
+    e2e_ms = dist_max(dist, e0.elapsed_ms(e1) / e2e_steps, local)
+    nat.call("pg_host_free", hp.value)
+    e2e_value = NTT_PER_STEP * world / (e2e_ms / 1e3)
+
+    peak, peak_kind = load_peaks()
+    achieved = ALGO_BYTES / (per_step / 1e3) / 1e9
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            import oracle as O  # the checker, timed as the CPU baseline only
+            v, sample, thr = cpu_reference(O.ntt_primes(1 << 50, 2 * N, L), seconds_target=args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+                   "sample": "C restatement of UintNttTable/DcrtPolynomial (oracle), OpenMP over rows; " + sample}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues, device generator)",
+            "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "ms_per_step": e2e_ms, "path": "pg_memcpy_h2d -> pg_dcrt_polymul_ntt_plain -> pg_memcpy_d2h"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": load_traffic(), "peak_source": peak_kind,
+                         "kernel": "ntt_cluster_kernel<16,13,4,RT> (fused fwd -> x plain -> inv)",
+                         "algorithmic_bytes_per_launch": ALGO_BYTES},
+            "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+                          "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="primus_b200", choices=["primus_b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

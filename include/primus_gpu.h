@@ -1,0 +1,205 @@
+/*
+ * primus_gpu.h -- C ABI of libprimus_gpu.so, the B200 (sm_100a) backend for
+ * the primus lattice-arithmetic path.
+ *
+ * The reference (serendipity-crypto/primus) is a Rust workspace with no FFI
+ * layer: its boundary is a set of traits and inherent methods.  Each entry
+ * point below names the reference item it replaces (crate/src/file.rs:line).
+ * A Rust `primus_gpu` crate binds these symbols with `extern "C"` and
+ * implements `NttTable` / `DcrtTable` on top of them.
+ *
+ * Conventions
+ *  - Every function returns an int status (PG_OK == 0); none aborts.  The
+ *    text of the last error on the calling thread is pg_last_error().
+ *  - Handles are library owned; data buffers are caller owned.
+ *  - `d_*` pointers are device pointers, `h_*` pointers host pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *  - Values are uint64_t.  A DCRT/CRT polynomial is limb-major [L][N]; a
+ *    batch of P polynomials is [P][L][N].  BigUint values are little-endian
+ *    limbs, coefficient-major [count][W].
+ *  - Canonical outputs are in [0, q).  Lazy forward outputs are in [0, 4q)
+ *    and equal the reference's lazy values bit for bit.
+ *  - Calls on distinct streams with disjoint buffers may run concurrently;
+ *    handles are immutable after creation and may be shared across threads.
+ */
+#ifndef PRIMUS_GPU_H
+#define PRIMUS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum {
+    PG_OK = 0,
+    PG_ERR_INVALID_ARGUMENT = 1,
+    PG_ERR_NO_PRIMITIVE_ROOT = 2,   /* NttError::NoPrimitiveRoot  (primus_ntt/src/error.rs:10-16) */
+    PG_ERR_DEGREE_TOO_LARGE = 3,    /* NttError::DegreeTooLarge   (primus_ntt/src/error.rs:26-33) */
+    PG_ERR_NOT_COPRIME = 4,         /* RNSError::CoPrimeError     (primus_rns/src/error.rs) */
+    PG_ERR_UNSUPPORTED = 5,         /* a size this build does not run */
+    PG_ERR_OUT_OF_MEMORY = 6,
+    PG_ERR_CUDA = 7,
+    PG_ERR_TIMEOUT = 8,             /* a bounded device wait ran out */
+    PG_ERR_REJECTED = 9             /* admission control refused a request */
+};
+
+const char *pg_status_string(int status);
+/* message of the last failing call on this thread ("" if none) */
+const char *pg_last_error(void);
+/* library version string and the compiled device architecture */
+const char *pg_version(void);
+
+/* ------------------------------------------------------- device utilities
+ * Thin wrappers so that hosts without a CUDA runtime binding (the Rust crate,
+ * ctypes) can manage buffers and streams. */
+int pg_device_count(int *count);
+int pg_set_device(int device);
+int pg_malloc(void **d_ptr, size_t bytes);
+int pg_free(void *d_ptr);
+int pg_host_alloc(void **h_ptr, size_t bytes); /* page-locked */
+int pg_host_free(void *h_ptr);
+int pg_memcpy_h2d(void *d_dst, const void *h_src, size_t bytes, void *stream);
+int pg_memcpy_d2h(void *h_dst, const void *d_src, size_t bytes, void *stream);
+int pg_memcpy_d2d(void *d_dst, const void *d_src, size_t bytes, void *stream);
+int pg_memset(void *d_ptr, int value, size_t bytes, void *stream);
+int pg_stream_create(void **stream);
+int pg_stream_destroy(void *stream);
+int pg_stream_synchronize(void *stream);
+int pg_device_synchronize(void);
+/* CUDA-event timing on a stream */
+int pg_event_create(void **event);
+int pg_event_destroy(void *event);
+int pg_event_record(void *event, void *stream);
+int pg_event_elapsed_ms(void *start, void *stop, float *ms);
+/* number of kernels this library has launched in this process */
+uint64_t pg_launch_count(void);
+
+/* --------------------------------------------------------- number theory
+ * Host helpers used to pick NTT-friendly primes the way the workloads do. */
+/* largest prime p < bound with p = 1 mod m (descending search, deterministic
+ * Miller-Rabin); 0 if none */
+uint64_t pg_prev_prime_congruent(uint64_t bound, uint64_t m);
+/* `count` descending primes below bound, each = 1 mod m */
+int pg_ntt_primes(uint64_t bound, uint64_t m, uint32_t count, uint64_t *h_out);
+/* minimal primitive 2^log_degree-th root of unity mod q
+ * (PrimitiveRoot::try_minimal_primitive_root, primus_ntt/src/root.rs:89-111) */
+int pg_minimal_primitive_root(uint32_t log_degree, uint64_t q, uint64_t *root);
+
+/* ------------------------------------------------------------- NTT tables
+ * One table holds L primes of one ring degree N = 2^log_n; L = 1 is the
+ * single-prime NttTable (primus_ntt/src/ntt/mod.rs:20-117), L > 1 the
+ * DcrtTable (primus_ntt/src/dcrt/mod.rs:17-129).  Twiddles (value + Shoup
+ * quotient), N^-1 and the monomial tables live in device memory until
+ * destroy.  Replaces UintNttTable::new (primitive.rs:113-185) and
+ * UintCrtNttTable::new (dcrt/primitive.rs:24-45). */
+typedef struct pg_ntt_table pg_ntt_table;
+
+int pg_ntt_table_create(uint32_t log_n, const uint64_t *h_moduli, uint32_t moduli_count,
+                        pg_ntt_table **out);
+int pg_ntt_table_destroy(pg_ntt_table *table);
+/* poly_length(), moduli_count(), crt_poly_length() */
+int pg_ntt_table_info(const pg_ntt_table *table, uint32_t *log_n, uint32_t *moduli_count,
+                      size_t *poly_length, size_t *crt_poly_length);
+/* host copies of limb `limb`'s tables: root, inv_root, inv_n and the
+ * bit-reversed root_powers / scrambled inv_root_powers (values and Shoup
+ * quotients, N each); any output may be NULL */
+int pg_ntt_table_export(const pg_ntt_table *table, uint32_t limb, uint64_t *root,
+                        uint64_t *inv_root, uint64_t *inv_n, uint64_t *h_root_powers,
+                        uint64_t *h_root_powers_q, uint64_t *h_inv_root_powers,
+                        uint64_t *h_inv_root_powers_q);
+/* the same tables computed on the host only, without a device (for checks) */
+int pg_ntt_host_tables(uint32_t log_n, uint64_t q, uint64_t *root, uint64_t *inv_root,
+                       uint64_t *inv_n, uint64_t *h_root_powers, uint64_t *h_root_powers_q,
+                       uint64_t *h_inv_root_powers, uint64_t *h_inv_root_powers_q);
+
+/* Forward NTT of `polys` DCRT polynomials in place ([polys][L][N]), natural
+ * order in ([0,4q)), bit-reversed order out: [0,4q) if lazy else [0,q).
+ * Replaces NttTable::lazy_transform_slice / transform_slice
+ * (primitive.rs:211-244) and DcrtTable::{lazy_,}transform_slice
+ * (dcrt/primitive.rs:96-115). */
+int pg_ntt_forward(const pg_ntt_table *table, uint64_t *d_data, size_t polys, int lazy,
+                   void *stream);
+/* Inverse NTT in place, bit-reversed in ([0,2q)), natural out ([0,q)).
+ * Replaces {lazy_,}inverse_transform_slice (primitive.rs:246-296,
+ * dcrt/primitive.rs:117-141). */
+int pg_ntt_inverse(const pg_ntt_table *table, uint64_t *d_data, size_t polys, int lazy,
+                   void *stream);
+/* Host-slice forms with the reference's exact call semantics (copy in,
+ * transform, copy out, synchronous). */
+int pg_ntt_forward_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
+int pg_ntt_inverse_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
+/* NTT of coeff*X^degree into every limb (coeff < every q), of X^degree and of
+ * -X^degree.  Replaces transform_monomial / transform_coeff_one_monomial /
+ * transform_coeff_minus_one_monomial (primitive.rs:298-397, dcrt/mod.rs:100-128). */
+int pg_ntt_monomial(const pg_ntt_table *table, uint64_t coeff, size_t degree, uint64_t *d_out,
+                    void *stream);
+int pg_ntt_coeff_one_monomial(const pg_ntt_table *table, size_t degree, uint64_t *d_out,
+                              void *stream);
+int pg_ntt_coeff_minus_one_monomial(const pg_ntt_table *table, size_t degree, uint64_t *d_out,
+                                    void *stream);
+
+/* ---------------------------------------------------- pointwise DCRT ops
+ * Element-wise over [polys][L][N] with limb l reduced mod moduli[l]; canonical
+ * inputs and outputs.  `rhs_polys` is polys or 1 (one rhs broadcast to every
+ * poly).  Replace DcrtPolynomial / ArrayBase ops in primus_poly. */
+/* x *= y        (DcrtPolynomial::mul_assign, primus_poly/src/dcrt/mul.rs:97-110) */
+int pg_dcrt_mul(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_y, size_t polys,
+                size_t rhs_polys, void *stream);
+/* x += y * z    (DcrtPolynomial::add_mul_assign, primus_poly/src/dcrt/mod.rs:94-114) */
+int pg_dcrt_add_mul(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_y,
+                    const uint64_t *d_z, size_t polys, size_t rhs_polys, void *stream);
+/* x += y, x -= y, x = -x (primus_poly/src/dcrt/{add,sub,neg}.rs) */
+int pg_dcrt_add(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_y, size_t polys,
+                size_t rhs_polys, void *stream);
+int pg_dcrt_sub(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_y, size_t polys,
+                size_t rhs_polys, void *stream);
+int pg_dcrt_neg(const pg_ntt_table *table, uint64_t *d_x, size_t polys, void *stream);
+/* x *= scalar[l] per limb (DcrtPolynomial::mul_scalar_assign, dcrt/mul.rs:27-34) */
+int pg_dcrt_mul_scalar(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *h_scalars,
+                       size_t polys, void *stream);
+/* x += y * scalar[l] (DcrtPolynomial::add_mul_scalar_assign, dcrt/mul.rs:37-58) */
+int pg_dcrt_add_mul_scalar(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_y,
+                           const uint64_t *h_scalars, size_t polys, void *stream);
+/* (a, b) = (a + s, (a - s) * w) with w a per-element Shoup factor
+ * polynomial (values d_w, quotients d_wq from pg_dcrt_shoup_prepare), one
+ * [L][N] w shared by every poly
+ * (DcrtPolynomial::butterfly_mul_factor_inplace, dcrt/mul.rs:119-155) */
+int pg_dcrt_butterfly_mul_factor(const pg_ntt_table *table, uint64_t *d_a, const uint64_t *d_s,
+                                 const uint64_t *d_w, const uint64_t *d_wq, uint64_t *d_b,
+                                 size_t polys, void *stream);
+/* Shoup quotients floor(v*2^64/q_l) of a [rhs_polys][L][N] operand, so that
+ * products against it take the one-mulhi Shoup path (ShoupFactor::new,
+ * primus_factor/src/shoup_factor/mod.rs:44-55) */
+int pg_dcrt_shoup_prepare(const pg_ntt_table *table, const uint64_t *d_values,
+                          uint64_t *d_quotients, size_t polys, void *stream);
+/* x *= (w, w') with Shoup-prepared rhs (DcrtPolynomial::mul_factor_assign
+ * element-wise form) */
+int pg_dcrt_mul_prepared(const pg_ntt_table *table, uint64_t *d_x, const uint64_t *d_w,
+                         const uint64_t *d_wq, size_t polys, size_t rhs_polys, void *stream);
+
+/* ------------------------------------------------- fused polynomial multiply
+ * For every row of [polys][L][N]: forward NTT, multiply by the NTT-domain
+ * plaintext (one [L][N] operand with its Shoup quotients from
+ * pg_dcrt_shoup_prepare), inverse NTT -- one launch, one HBM read and one
+ * write per row.  Output equals transform_slice -> DcrtPolynomial::mul_assign
+ * -> inverse_transform_slice (the reference's three calls) bit for bit. */
+int pg_dcrt_polymul_ntt_plain(const pg_ntt_table *table, uint64_t *d_data,
+                              const uint64_t *d_plain, const uint64_t *d_plain_q, size_t polys,
+                              void *stream);
+
+/* ------------------------------------------------------- seeded inputs
+ * Device-side fill with the counter-based generator (uniform below q_l per
+ * limb; stream id = stream0 + poly*L + limb). */
+int pg_fill_uniform(const pg_ntt_table *table, uint64_t *d_out, size_t polys, uint64_t seed,
+                    uint64_t stream0, void *stream);
+/* host form of the same generator: out[i] for i < n, uniform below q */
+int pg_fill_uniform_host(uint64_t seed, uint64_t stream_id, uint64_t q, size_t n,
+                         uint64_t *h_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRIMUS_GPU_H */

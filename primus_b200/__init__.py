@@ -1,0 +1,16 @@
+"""primus_b200: B200-native (sm_100a) backend for the primus lattice-arithmetic path.
+
+The compute lives in libprimus_gpu.so (hand-written CUDA, C ABI in
+include/primus_gpu.h); this package is the host-side mirror of the reference's
+trait API.  Importing it loads the library and fails loudly when it is absent.
+"""
+from ._native import (DeviceBuffer, Event, PrimusGpuError, Stream, device_count, launch_count,  # noqa: F401
+                      synchronize)
+from .ntt import (DcrtTable, NttError, NttTable, host_tables, minimal_primitive_root,  # noqa: F401
+                  ntt_primes, prev_prime_congruent)
+
+__all__ = [
+    "DcrtTable", "NttTable", "NttError", "DeviceBuffer", "Stream", "Event", "PrimusGpuError",
+    "ntt_primes", "prev_prime_congruent", "minimal_primitive_root", "host_tables", "device_count",
+    "launch_count", "synchronize",
+]

@@ -1,0 +1,111 @@
+// Device-side modular arithmetic shared by every kernel of libprimus_gpu.
+//
+// All arithmetic is exact unsigned 64/128-bit integer math.  The Shoup lazy
+// multiply is the reference's ShoupFactor::lazy_factor_mul_modulo
+// (primus_factor/src/shoup_factor/mod.rs:108-113): w*b - q*hi64(w'*b), which
+// lands in [0, 2q) for any 64-bit b.  Because the same formula is evaluated on
+// the same operands, lazy intermediate values match the CPU path bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define PG_DEV __device__ __forceinline__
+#define PG_HD __host__ __device__ __forceinline__
+
+namespace pg {
+
+// hi 64 bits of a 64x64 product
+PG_DEV uint64_t mulhi64(uint64_t a, uint64_t b) { return __umul64hi(a, b); }
+
+// Shoup lazy multiply: result in [0, 2q)
+PG_DEV uint64_t shoup_lazy(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {
+    return w * b - q * mulhi64(wq, b);
+}
+
+// Shoup full multiply: result in [0, q)
+PG_DEV uint64_t shoup_mul(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {
+    uint64_t t = shoup_lazy(w, wq, b, q);
+    return t >= q ? t - q : t;
+}
+
+PG_DEV uint64_t reduce_once(uint64_t v, uint64_t m) { return v >= m ? v - m : v; }
+
+// UintModulus::reduce_add (primus_modulus/src/unsigned_integer/ops.rs:34-41)
+PG_DEV uint64_t add_mod(uint64_t a, uint64_t b, uint64_t m) {
+    uint64_t s = a + b;
+    return s >= m ? s - m : s;
+}
+
+// UintModulus::reduce_sub (ops.rs:81-87)
+PG_DEV uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t m) { return b > a ? a - b + m : a - b; }
+
+// UintModulus::reduce_neg (ops.rs:105-111)
+PG_DEV uint64_t neg_mod(uint64_t a, uint64_t m) { return a == 0 ? 0 : m - a; }
+
+// Exact (a*b + c) mod q for q < 2^62 via Barrett with ratio = floor(2^128/q)
+// (BarrettModulus, primus_modulus/src/barrett/ops.rs:41-76, 342-355).  The
+// output is canonical, so it equals the CPU path's value for any exact method.
+struct Barrett {
+    uint64_t q, r0, r1;  // ratio = r1*2^64 + r0
+};
+
+PG_DEV uint64_t barrett_reduce_2limb(uint64_t lo, uint64_t hi, const Barrett& m) {
+    uint64_t ah = mulhi64(lo, m.r0);
+    // b = lo*r1 + ah (128-bit)
+    uint64_t b0 = lo * m.r1;
+    uint64_t b1 = mulhi64(lo, m.r1);
+    b0 += ah;
+    b1 += (b0 < ah);
+    // c = hi*r0 (128-bit)
+    uint64_t c0 = hi * m.r0;
+    uint64_t c1 = mulhi64(hi, m.r0);
+    uint64_t s = b0 + c0;
+    uint64_t carry = s < b0;
+    uint64_t qq = hi * m.r1 + b1 + c1 + carry;
+    uint64_t r = lo - qq * m.q;
+    // lazy result is in [0, 3q) at worst for q < 2^62; two conditional subtracts
+    r = r >= m.q ? r - m.q : r;
+    return r >= m.q ? r - m.q : r;
+}
+
+PG_DEV uint64_t barrett_mul(uint64_t a, uint64_t b, const Barrett& m) {
+    return barrett_reduce_2limb(a * b, mulhi64(a, b), m);
+}
+
+PG_DEV uint64_t barrett_mul_add(uint64_t a, uint64_t b, uint64_t c, const Barrett& m) {
+    uint64_t lo = a * b;
+    uint64_t hi = mulhi64(a, b);
+    lo += c;
+    hi += (lo < c);
+    return barrett_reduce_2limb(lo, hi, m);
+}
+
+// Counter-based seeded generator (identical to the host generator): a 64-bit
+// hash of (seed, stream, index, attempt); uniform values below q by rejection
+// on the top bitlen(q-1) bits.
+PG_HD uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+PG_HD uint64_t hash64(uint64_t seed, uint64_t stream, uint64_t index, uint64_t attempt) {
+    uint64_t h = mix64(seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull);
+    h = mix64(h ^ (stream * 0xD1B54A32D192ED03ull));
+    h = mix64(h ^ (index * 0xA0761D6478BD642Full) ^ (attempt * 0xE7037ED1A0B428DBull));
+    return h;
+}
+
+PG_DEV uint64_t uniform_at(uint64_t seed, uint64_t stream, uint64_t index, uint64_t q) {
+    if (q <= 1) return 0;
+    int bits = 64 - __clzll(q - 1);
+    // rejection accepts with probability > 1/2; 64 attempts bound the loop
+    for (uint64_t attempt = 0; attempt < 64; ++attempt) {
+        uint64_t v = hash64(seed, stream, index, attempt) >> (64 - bits);
+        if (v < q) return v;
+    }
+    return 0;
+}
+
+}  // namespace pg

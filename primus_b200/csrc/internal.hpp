@@ -1,0 +1,112 @@
+// Internal declarations shared by the translation units of libprimus_gpu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/primus_gpu.h"
+#include "common.cuh"
+
+namespace pg {
+
+// ---- error handling: every entry point returns a status and records a message
+int set_error(int status, const std::string& msg);
+int cuda_status(cudaError_t err, const char* what);
+void clear_error();
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+#define PG_CUDA(expr)                                              \
+    do {                                                           \
+        cudaError_t _e = (expr);                                   \
+        if (_e != cudaSuccess) return ::pg::cuda_status(_e, #expr); \
+    } while (0)
+
+#define PG_LAUNCH_CHECK(what)                                        \
+    do {                                                             \
+        cudaError_t _e = cudaGetLastError();                         \
+        if (_e != cudaSuccess) return ::pg::cuda_status(_e, what);   \
+    } while (0)
+
+// ---- host number theory (exact, unsigned __int128)
+using u128 = unsigned __int128;
+uint64_t h_mulmod(uint64_t a, uint64_t b, uint64_t q);
+uint64_t h_powmod(uint64_t a, uint64_t e, uint64_t q);
+uint64_t h_invmod(uint64_t a, uint64_t q);
+bool h_is_prime(uint64_t n);
+inline uint64_t h_shoup_quotient(uint64_t w, uint64_t q) { return (uint64_t)(((u128)w << 64) / q); }
+inline uint64_t h_shoup_mul(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {
+    uint64_t hw = (uint64_t)(((u128)wq * b) >> 64);
+    uint64_t t = w * b - q * hw;
+    return t >= q ? t - q : t;
+}
+Barrett h_barrett(uint64_t q);
+
+// Host copy of one prime's tables (UintNttTable, primus_ntt/src/ntt/primitive.rs:34-46)
+struct HostNttTable {
+    uint64_t q = 0, root = 0, inv_root = 0, inv_n = 0, inv_n_q = 0;
+    uint32_t log_n = 0;
+    std::vector<uint64_t> root_powers, root_powers_q;          // [N] bit-reversed
+    std::vector<uint64_t> inv_root_powers, inv_root_powers_q;  // [N] scrambled
+    std::vector<uint64_t> ordinal, ordinal_q;                  // [2N]
+};
+int build_host_table(uint32_t log_n, uint64_t q, HostNttTable& t);
+
+}  // namespace pg
+
+// Device-resident table set for L primes of degree N = 2^log_n.
+struct pg_ntt_table {
+    uint32_t log_n = 0, L = 0;
+    size_t n = 0;
+    int device = 0;
+    std::vector<uint64_t> moduli;
+    std::vector<pg::HostNttTable> host;
+    uint64_t* d_moduli = nullptr;      // [L]
+    ulonglong2* d_fwd = nullptr;       // [L][N] (w, w') bit-reversed root powers
+    ulonglong2* d_inv = nullptr;       // [L][N] (w, w') scrambled inverse powers
+    ulonglong2* d_ordinal = nullptr;   // [L][2N] psi^k
+    ulonglong2* d_inv_n = nullptr;     // [L] N^-1
+    ulonglong2* d_inv_last = nullptr;  // [L] inv_root_powers[N-1] * N^-1
+    pg::Barrett* d_barrett = nullptr;  // [L]
+};
+
+namespace pg {
+// kernel argument block for the NTT family
+struct NttArgs {
+    uint64_t* data;
+    const ulonglong2* fwd;
+    const ulonglong2* inv;
+    const uint64_t* moduli;
+    const ulonglong2* inv_n;
+    const ulonglong2* inv_last;
+    const uint64_t* plain;
+    const uint64_t* plain_q;
+    uint64_t rows;
+    uint32_t L;
+    int lazy;
+};
+
+enum NttMode { MODE_FWD = 0, MODE_INV = 1, MODE_RT = 2 };
+
+inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, int lazy) {
+    NttArgs a{};
+    a.data = data;
+    a.fwd = t->d_fwd;
+    a.inv = t->d_inv;
+    a.moduli = t->d_moduli;
+    a.inv_n = t->d_inv_n;
+    a.inv_last = t->d_inv_last;
+    a.plain = nullptr;
+    a.plain_q = nullptr;
+    a.rows = rows;
+    a.L = t->L;
+    a.lazy = lazy;
+    return a;
+}
+
+int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
+}  // namespace pg

@@ -1,0 +1,660 @@
+// Negacyclic NTT / INTT kernels for sm_100a.
+//
+// Semantics: the reference's UintNttTable (primus_ntt/src/ntt/primitive.rs).
+//   forward  (lazy_transform_slice :211-232): for gap = N/2 .. 1, chunk c of
+//            size 2*gap uses root_powers[2^s + c] (s = stage); Harvey
+//            butterfly u = x mod 2q; v = w*y (Shoup lazy); x = u+v; y = u+2q-v.
+//   inverse  (lazy_inverse_transform_slice :246-286): for gap = 1 .. N/4,
+//            GS butterfly with inv_root_powers read sequentially; the last
+//            stage (gap N/2) is fused with the N^-1 scaling.
+// Every butterfly is evaluated with the reference's formula on the same
+// operands and stages run in the reference's order, so lazy outputs match the
+// CPU values bit for bit.  Only the assignment of butterflies to threads
+// differs.
+//
+// Layout and schedule (B200):
+//   * N <= 2^13: one CTA owns one row (or several small rows) in shared memory.
+//     Each thread holds E = 2^LOG_E elements in registers and runs LOG_E stages
+//     per round; rounds exchange through padded shared memory (index i is
+//     stored at i + i/16, which keeps 64-bit accesses within two-way bank
+//     conflicts for every round).
+//   * N = 2^14 .. 2^16: a thread-block cluster of C = N / 2^13 CTAs owns one
+//     row (512 KiB at N = 2^16) in distributed shared memory.  Forward: the
+//     first log2(C) stages pair elements 2^13 apart, so each CTA takes a slab
+//     of columns {l + 2^13 j}, runs those stages in registers and scatters the
+//     results to the owning CTA's shared memory (st.shared::cluster); the
+//     remaining 13 stages are local.  Inverse mirrors this.  A row is read from
+//     and written to HBM exactly once, also for the fused fwd -> x plain -> inv
+//     round trip.
+#include <cooperative_groups.h>
+
+#include "internal.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace pg {
+
+PG_DEV int padi(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded(int m) { return m + (m >> 4); }
+
+template <int V>
+struct IC {
+    static constexpr int value = V;
+};
+
+// compile-time loop: f(IC<B>), f(IC<B+1>), ..., f(IC<E_-1>); every index is a
+// constant, so register arrays indexed by it stay in registers
+template <int B, int E_, typename F>
+PG_DEV void static_for(F&& f) {
+    if constexpr (B < E_) {
+        f(IC<B>{});
+        static_for<B + 1, E_>(f);
+    }
+}
+
+// Harvey forward butterfly; x, y in [0, 4q) -> [0, 4q)
+PG_DEV void fwd_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t q2) {
+    uint64_t u = x >= q2 ? x - q2 : x;
+    uint64_t v = shoup_lazy(w.x, w.y, y, q);
+    x = u + v;
+    y = u + q2 - v;
+}
+
+// Gentleman-Sande inverse butterfly; x, y in [0, 2q) -> [0, 2q)
+PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t q2) {
+    uint64_t u = x, v = y;
+    uint64_t s = u + v;
+    x = s >= q2 ? s - q2 : s;
+    y = shoup_lazy(w.x, w.y, u + q2 - v, q);
+}
+
+// Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+2q-v), canonical
+PG_DEV void inv_last_bfly(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, uint64_t q,
+                          uint64_t q2) {
+    uint64_t u = x, v = y;
+    x = shoup_mul(s.x, s.y, u + v, q);
+    y = shoup_mul(sr.x, sr.y, u + q2 - v, q);
+}
+
+PG_DEV uint64_t canon4(uint64_t v, uint64_t q, uint64_t q2) {
+    v = v >= q2 ? v - q2 : v;
+    return v >= q ? v - q : v;
+}
+
+// insert LOG_E zero bits at bit position g into t
+template <int LOG_E>
+PG_DEV uint32_t group_base(uint32_t t, int g) {
+    uint32_t lo = t & ((1u << g) - 1u);
+    return ((t >> g) << (g + LOG_E)) | lo;
+}
+
+// One forward round over register group x (x[jj] is local index base + (jj << G)).
+// Stage bits P_HI down to P_LO of an M = 2^LOG_M block whose twiddle row base
+// is tw_base (= C + cluster rank; 1 for a whole row): stage bit p uses
+// tw[(tw_base << (LOG_M-1-p)) + (i >> (p+1))].
+template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO>
+PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
+                      uint64_t q, uint64_t q2) {
+    constexpr int E = 1 << LOG_E;
+    static_for<0, P_HI - P_LO + 1>([&](auto it) {
+        constexpr int p = P_HI - decltype(it)::value;
+        constexpr int r = p - G;
+        constexpr int half = 1 << r;
+        constexpr int sp = LOG_M - 1 - p;
+        const uint32_t row0 = (tw_base << sp) + (base >> (p + 1));
+        static_for<0, (E >> (r + 1))>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            const ulonglong2 w = __ldg(tw + row0 + k);
+            static_for<0, half>([&](auto ll) {
+                constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
+                fwd_bfly(x[jj], x[jj + half], w, q, q2);
+            });
+        });
+    });
+}
+
+// One inverse round, stage bits P_LO up to P_HI (gap 2^p).  The element at
+// local index i of CTA rank `rank` has global index rank*M + i; stage p uses
+// inv[N + 1 - (N >> p) + ((rank*M + i) >> (p+1))].  If the last stage of the
+// whole transform (p == LOG_N-1) falls inside the round it is the scaled one.
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI>
+PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
+                      ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t q2) {
+    constexpr int E = 1 << LOG_E;
+    constexpr uint32_t N = 1u << LOG_N;
+    static_for<0, P_HI - P_LO + 1>([&](auto it) {
+        constexpr int p = P_LO + decltype(it)::value;
+        constexpr int r = p - G;
+        constexpr int half = 1 << r;
+        if constexpr (p == LOG_N - 1) {
+            static_for<0, E>([&](auto jt) {
+                constexpr int jj = decltype(jt)::value;
+                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, q2);
+            });
+        } else {
+            const uint32_t row0 = N + 1 - (N >> p) + (((rank << LOG_M) + base) >> (p + 1));
+            static_for<0, (E >> (r + 1))>([&](auto kk) {
+                constexpr int k = decltype(kk)::value;
+                const ulonglong2 w = __ldg(itw + row0 + k);
+                static_for<0, half>([&](auto ll) {
+                    constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
+                    inv_bfly(x[jj], x[jj + half], w, q, q2);
+                });
+            });
+        }
+    });
+}
+
+template <int LOG_E, int G>
+PG_DEV void load_smem(uint64_t (&x)[1 << LOG_E], const uint64_t* sm, uint32_t base) {
+#pragma unroll
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) x[jj] = sm[padi(base + ((uint32_t)jj << G))];
+}
+
+template <int LOG_E, int G>
+PG_DEV void store_smem(const uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t base) {
+#pragma unroll
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) sm[padi(base + ((uint32_t)jj << G))] = x[jj];
+}
+
+// ---- forward rounds 1.. over a block in shared memory (round 0 done by caller)
+template <int LOG_M, int LOG_E, int R>
+struct FwdRounds {
+    // round R processes bits [P_LO, P_HI]; its group spans [P_LO, P_LO + LOG_E)
+    static constexpr int P_HI = LOG_M - 1 - R * LOG_E;
+    static constexpr int P_LO = (P_HI - LOG_E + 1) > 0 ? (P_HI - LOG_E + 1) : 0;
+    static constexpr int G = P_LO;
+    static constexpr bool LAST = (P_LO == 0);
+};
+
+// Runs forward rounds R..last on x (x holds round R-1's group on entry, which
+// is stored to smem first).  On exit x holds the last round's group (G = 0,
+// i.e. E contiguous elements starting at tid*E).
+template <int LOG_M, int LOG_E, int R>
+PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
+                     const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2) {
+    using Cur = FwdRounds<LOG_M, LOG_E, R>;
+    using Prev = FwdRounds<LOG_M, LOG_E, R - 1>;
+    store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+    __syncthreads();
+    const uint32_t base = group_base<LOG_E>(tid, Cur::G);
+    load_smem<LOG_E, Cur::G>(x, sm, base);
+    fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO>(x, base, tw_base, tw, q, q2);
+    if constexpr (!Cur::LAST) fwd_rest<LOG_M, LOG_E, R + 1>(x, sm, tid, tw_base, tw, q, q2);
+}
+
+template <int LOG_M, int LOG_E, int R>
+struct InvRounds {
+    static constexpr int P_LO = R * LOG_E;
+    static constexpr int P_HI = (P_LO + LOG_E - 1) < (LOG_M - 1) ? (P_LO + LOG_E - 1) : (LOG_M - 1);
+    static constexpr int G = P_LO < (LOG_M - LOG_E) ? P_LO : (LOG_M - LOG_E);
+    static constexpr bool LAST = (P_HI == LOG_M - 1);
+};
+
+// Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
+// (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
+template <int LOG_N, int LOG_M, int LOG_E, int R, int R_END>
+PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
+                      const ulonglong2* __restrict__ itw, ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t q2) {
+    if constexpr (R < R_END) {
+        using Cur = InvRounds<LOG_M, LOG_E, R>;
+        using Prev = InvRounds<LOG_M, LOG_E, R - 1>;
+        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+        __syncthreads();
+        const uint32_t base = group_base<LOG_E>(tid, Cur::G);
+        load_smem<LOG_E, Cur::G>(x, sm, base);
+        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, s, sr, q, q2);
+        inv_range<LOG_N, LOG_M, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, s, sr, q, q2);
+    }
+}
+
+// ============================================================================
+// Single-CTA kernel: ROWS rows of N = 2^LOG_N per CTA, T = N/E threads per row.
+// ============================================================================
+template <int LOG_N, int LOG_E, int ROWS, int MODE>
+__global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kernel(NttArgs a) {
+    constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E;
+    extern __shared__ uint64_t smem_block[];
+    const uint32_t tid = threadIdx.x;
+    const uint64_t row = (uint64_t)blockIdx.x * ROWS + threadIdx.y;
+    const bool active = row < a.rows;
+    const uint32_t limb = (uint32_t)((active ? row : 0) % a.L);
+    uint64_t* sm = smem_block + threadIdx.y * padded(N);
+    uint64_t* g = a.data + (active ? row : 0) * N;
+    const uint64_t q = a.moduli[limb], q2 = q << 1;
+    uint64_t x[E];
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        using R0 = FwdRounds<LOG_N, LOG_E, 0>;
+        // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = active ? g[tid + jj * T] : 0;
+        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO>(x, tid, 1, tw, q, q2);
+        if constexpr (!R0::LAST) fwd_rest<LOG_N, LOG_E, 1>(x, sm, tid, 1, tw, q, q2);
+        // x = E contiguous outputs at tid*E
+        if constexpr (MODE == MODE_FWD) {
+            if (!a.lazy) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
+            }
+            __syncthreads();
+            store_smem<LOG_E, 0>(x, sm, tid * E);
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < E; ++k) g[tid + k * T] = sm[padi(tid + k * T)];
+            }
+            return;
+        } else {
+            // pointwise product with the NTT-domain plaintext (Shoup-prepared)
+            const uint64_t* pv = a.plain + (size_t)limb * N + tid * E;
+            const uint64_t* pq = a.plain_q + (size_t)limb * N + tid * E;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_mul(__ldg(pv + jj), __ldg(pq + jj), canon4(x[jj], q, q2), q);
+        }
+    }
+    // ---------------- inverse
+    if constexpr (MODE != MODE_FWD) {
+        const ulonglong2* itw = a.inv + (size_t)limb * N;
+        const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
+        using I0 = InvRounds<LOG_N, LOG_E, 0>;
+        if constexpr (MODE == MODE_INV) {
+            // stage the bit-reversed row through smem (coalesced), then round 0
+#pragma unroll
+            for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = active ? g[tid + k * T] : 0;
+            __syncthreads();
+            load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
+        } else {
+            // round trip: the forward's last group (tid*E .. tid*E+E-1) is the
+            // inverse's first group whenever LOG_N >= LOG_E (I0::G == 0)
+            static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
+            __syncthreads();  // all forward smem reads done before inverse smem writes
+        }
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, s, sr, q,
+                                                                  q2);
+        inv_range<LOG_N, LOG_N, LOG_E, 1, (LOG_N + LOG_E - 1) / LOG_E>(x, sm, tid, 0, itw, s, sr, q, q2);
+        // last group: elements tid + jj*T, coalesced store
+        using Last = InvRounds<LOG_N, LOG_E, (LOG_N + LOG_E - 1) / LOG_E - 1>;
+        static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
+        if (active) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) g[tid + jj * T] = x[jj];
+        }
+    }
+}
+
+// ============================================================================
+// Cluster kernel: a row of N = 2^LOG_N is owned by C = 2^(LOG_N - LOG_M) CTAs.
+// CTA `rank` owns the contiguous block [rank*M, (rank+1)*M) for the local
+// stages and the column slab [rank*M/C, (rank+1)*M/C) for the cross stages.
+// ============================================================================
+PG_DEV void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
+PG_DEV void cluster_arrive_release() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+PG_DEV void cluster_wait_acquire() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
+PG_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// st.shared::cluster of one u64 into CTA `rank`'s shared memory at the same offset
+PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(remote) : "r"(local_addr), "r"(rank));
+    asm volatile("st.shared::cluster.u64 [%0], %1;\n" ::"r"(remote), "l"(v) : "memory");
+}
+
+template <int LOG_N, int LOG_M, int LOG_E, int MODE>
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttArgs a) {
+    constexpr int LOG_C = LOG_N - LOG_M;
+    constexpr int N = 1 << LOG_N, M = 1 << LOG_M, C = 1 << LOG_C, E = 1 << LOG_E, T = M / E;
+    constexpr int K = E / C;       // columns per thread in the cross stages
+    constexpr int SLAB = M / C;    // columns per CTA
+    static_assert(K >= 1 && K * T == SLAB, "column split");
+    extern __shared__ uint64_t smem_cl[];
+    uint64_t* sm = smem_cl;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t rank = blockIdx.x & (C - 1);
+    const uint64_t row = blockIdx.x >> LOG_C;  // grid is exactly rows * C
+    const uint32_t limb = (uint32_t)(row % a.L);
+    uint64_t* g = a.data + row * N;
+    const uint64_t q = a.moduli[limb], q2 = q << 1;
+    const uint32_t col0 = rank * SLAB + tid * K;  // first column of this thread
+    uint64_t x[E];
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        cluster_arrive_relaxed();  // matched by the wait before the first remote store
+        // cross stages on columns: x[k*C + j] = row[col0 + k + j*M]
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < C; ++j) x[k * C + j] = g[col0 + k + j * M];
+        static_for<0, LOG_C>([&](auto st) {
+            constexpr int stg = decltype(st)::value;
+            constexpr int p = LOG_C - 1 - stg;  // bit of j
+            constexpr int half = 1 << p;
+            static_for<0, (C >> (p + 1))>([&](auto jt) {
+                constexpr int jc = decltype(jt)::value;
+                const ulonglong2 w = __ldg(tw + (1 << stg) + jc);
+                static_for<0, K>([&](auto kt) {
+                    constexpr int k = decltype(kt)::value;
+                    static_for<0, half>([&](auto lt) {
+                        constexpr int j = (jc << (p + 1)) | decltype(lt)::value;
+                        fwd_bfly(x[k * C + j], x[k * C + j + half], w, q, q2);
+                    });
+                });
+            });
+        });
+        cluster_wait_acquire();  // every CTA of the cluster is running
+        // scatter: element (column c, j) -> CTA j, local index c
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < C; ++j) st_cluster(smem_u32(sm + padi(col0 + k)), j, x[k * C + j]);
+        cluster_arrive_release();
+        cluster_wait_acquire();
+        // local stages: round 0 from smem, then the rest
+        using R0 = FwdRounds<LOG_M, LOG_E, 0>;
+        load_smem<LOG_E, R0::G>(x, sm, group_base<LOG_E>(tid, R0::G));
+        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO>(x, group_base<LOG_E>(tid, R0::G), C + rank, tw, q, q2);
+        fwd_rest<LOG_M, LOG_E, 1>(x, sm, tid, C + rank, tw, q, q2);
+        if constexpr (MODE == MODE_FWD) {
+            if (!a.lazy) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
+            }
+            __syncthreads();
+            store_smem<LOG_E, 0>(x, sm, tid * E);
+            __syncthreads();
+            uint64_t* gb = g + rank * M;
+#pragma unroll
+            for (int k = 0; k < E; ++k) gb[tid + k * T] = sm[padi(tid + k * T)];
+            return;
+        } else {
+            const uint64_t* pv = a.plain + (size_t)limb * N + rank * M + tid * E;
+            const uint64_t* pq = a.plain_q + (size_t)limb * N + rank * M + tid * E;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_mul(__ldg(pv + jj), __ldg(pq + jj), canon4(x[jj], q, q2), q);
+            __syncthreads();
+        }
+    }
+    // ---------------- inverse
+    if constexpr (MODE == MODE_FWD) return;
+    const ulonglong2* itw = a.inv + (size_t)limb * N;
+    const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
+    using I0 = InvRounds<LOG_M, LOG_E, 0>;
+    if constexpr (MODE == MODE_INV) {
+        uint64_t* gb = g + rank * M;
+#pragma unroll
+        for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = gb[tid + k * T];
+        __syncthreads();
+        load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
+    }
+    inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, s, sr, q,
+                                                              q2);
+    // rounds 1..last: the last round's smem loads are followed by the cluster
+    // arrive so that no CTA overwrites a block another CTA is still reading
+    using ILast = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 1>;
+    static_assert(ILast::G == LOG_M - LOG_E, "last local inverse group");
+    static_assert((LOG_M + LOG_E - 1) / LOG_E >= 2, "cluster path needs two local rounds");
+    inv_range<LOG_N, LOG_M, LOG_E, 1, (LOG_M + LOG_E - 1) / LOG_E - 1>(x, sm, tid, rank, itw, s, sr, q, q2);
+    {
+        using Prev = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 2>;
+        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+        __syncthreads();
+        const uint32_t base = group_base<LOG_E>(tid, ILast::G);  // == tid
+        load_smem<LOG_E, ILast::G>(x, sm, base);
+        cluster_arrive_relaxed();
+        inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, s, sr, q, q2);
+        cluster_wait_acquire();
+        // element local index tid + jj*T (column c = that index) -> CTA c / SLAB,
+        // column buffer slot [rank][c % SLAB]
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) {
+            const uint32_t c = tid + jj * T;
+            st_cluster(smem_u32(sm + padi(rank * SLAB + (c & (SLAB - 1)))), c / SLAB, x[jj]);
+        }
+        cluster_arrive_release();
+        cluster_wait_acquire();
+    }
+    // cross inverse stages on columns col0 + k: x[k*C + j] = element col0 + k + j*M
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < C; ++j) x[k * C + j] = sm[padi(j * SLAB + tid * K + k)];
+    static_for<0, LOG_C>([&](auto pt) {
+        constexpr int pp = decltype(pt)::value;  // global stage LOG_M + pp, bit pp of j
+        constexpr int half = 1 << pp;
+        constexpr int stage = LOG_M + pp;
+        if constexpr (stage == LOG_N - 1) {
+            static_for<0, K>([&](auto kt) {
+                constexpr int k = decltype(kt)::value;
+                static_for<0, C>([&](auto jt) {
+                    constexpr int j = decltype(jt)::value;
+                    if constexpr (!(j & half)) inv_last_bfly(x[k * C + j], x[k * C + j + half], s, sr, q, q2);
+                });
+            });
+        } else {
+            static_for<0, (C >> (pp + 1))>([&](auto jt) {
+                constexpr int jc = decltype(jt)::value;
+                const ulonglong2 w = __ldg(itw + (N + 1 - (N >> stage)) + jc);
+                static_for<0, K>([&](auto kt) {
+                    constexpr int k = decltype(kt)::value;
+                    static_for<0, half>([&](auto lt) {
+                        constexpr int j = (jc << (pp + 1)) | decltype(lt)::value;
+                        inv_bfly(x[k * C + j], x[k * C + j + half], w, q, q2);
+                    });
+                });
+            });
+        }
+    });
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < C; ++j) g[col0 + k + j * M] = x[k * C + j];
+}
+
+}  // namespace pg
+
+// ============================================================================
+// Launch dispatch
+// ============================================================================
+namespace pg {
+
+template <int LOG_N, int LOG_E, int ROWS, int MODE>
+static int launch_block(const NttArgs& a, cudaStream_t st) {
+    constexpr int T = 1 << (LOG_N - LOG_E);
+    constexpr size_t smem = (size_t)ROWS * padded(1 << LOG_N) * sizeof(uint64_t);
+    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return cuda_status(attr, "ntt_block_kernel: shared memory attribute");
+    dim3 block(T, ROWS);
+    dim3 grid((unsigned)((a.rows + ROWS - 1) / ROWS));
+    kern<<<grid, block, smem, st>>>(a);
+    count_launch();
+    PG_LAUNCH_CHECK("ntt_block_kernel launch");
+    return PG_OK;
+}
+
+template <int LOG_N, int LOG_M, int LOG_E, int MODE>
+static int launch_cluster(const NttArgs& a, cudaStream_t st) {
+    constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
+    constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
+    if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.rows * C));
+    cfg.blockDim = dim3(T);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    count_launch();
+    if (e != cudaSuccess) return cuda_status(e, "ntt_cluster_kernel launch");
+    return PG_OK;
+}
+
+template <int MODE>
+static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
+    switch (log_n) {
+        case 1: return launch_block<1, 1, 128, MODE>(a, st);
+        case 2: return launch_block<2, 2, 128, MODE>(a, st);
+        case 3: return launch_block<3, 3, 128, MODE>(a, st);
+        case 4: return launch_block<4, 3, 64, MODE>(a, st);
+        case 5: return launch_block<5, 3, 32, MODE>(a, st);
+        case 6: return launch_block<6, 3, 16, MODE>(a, st);
+        case 7: return launch_block<7, 3, 8, MODE>(a, st);
+        case 8: return launch_block<8, 3, 4, MODE>(a, st);
+        case 9: return launch_block<9, 3, 2, MODE>(a, st);
+        case 10: return launch_block<10, 3, 1, MODE>(a, st);
+        case 11: return launch_block<11, 3, 1, MODE>(a, st);
+        case 12: return launch_block<12, 4, 1, MODE>(a, st);
+        case 13: return launch_block<13, 4, 1, MODE>(a, st);
+        case 14: return launch_cluster<14, 13, 4, MODE>(a, st);
+        case 15: return launch_cluster<15, 13, 4, MODE>(a, st);
+        case 16: return launch_cluster<16, 13, 4, MODE>(a, st);
+        default: return set_error(PG_ERR_UNSUPPORTED, "this build runs NTTs for log_n in [1, 16]");
+    }
+}
+
+int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
+    if (a.rows == 0) return PG_OK;
+    switch (mode) {
+        case MODE_FWD: return launch_mode<MODE_FWD>(a, log_n, st);
+        case MODE_INV: return launch_mode<MODE_INV>(a, log_n, st);
+        case MODE_RT: return launch_mode<MODE_RT>(a, log_n, st);
+    }
+    return set_error(PG_ERR_INVALID_ARGUMENT, "bad NTT mode");
+}
+
+// ---------------------------------------------------------------- monomials
+// transform_monomial (primus_ntt/src/ntt/primitive.rs:298-349): out[i] =
+// coeff * psi^((2 rev(i) + 1) * degree mod 2N); kind 0 = general coeff,
+// 1 = X^degree, 2 = -X^degree (index XOR N selects -psi^k).
+__global__ void monomial_kernel(uint64_t* out, const ulonglong2* __restrict__ ordinal, const uint64_t* __restrict__ moduli,
+                                uint32_t log_n, uint32_t L, uint64_t coeff, uint64_t degree, int kind) {
+    const size_t n = (size_t)1 << log_n;
+    const size_t total = n * L;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t l = (uint32_t)(idx >> log_n);
+        const uint32_t i = (uint32_t)(idx & (n - 1));
+        const uint64_t q = moduli[l];
+        uint64_t v;
+        if (kind == 0 && coeff == 0) {
+            v = 0;
+        } else if (degree == 0) {
+            v = kind == 0 ? coeff : (kind == 1 ? 1 : q - 1);
+        } else {
+            const uint32_t rev = __brev(i) >> (32 - log_n);
+            size_t e = ((2 * (size_t)rev + 1) * degree) & (2 * n - 1);
+            const ulonglong2* o = ordinal + (size_t)l * 2 * n;
+            if (kind == 2 || (kind == 0 && coeff == q - 1)) {
+                v = o[e ^ n].x;
+            } else if (kind == 1 || coeff == 1) {
+                v = o[e].x;
+            } else {
+                v = shoup_mul(o[e].x, o[e].y, coeff, q);
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+static int launch_monomial(const pg_ntt_table* t, uint64_t coeff, size_t degree, uint64_t* d_out, int kind,
+                           cudaStream_t st) {
+    if (!t || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL table or output");
+    if (degree >= t->n) return set_error(PG_ERR_INVALID_ARGUMENT, "degree must be below N");
+    const size_t total = t->n * t->L;
+    const unsigned threads = 256;
+    const unsigned blocks = (unsigned)std::min<size_t>((total + threads - 1) / threads, 148 * 16);
+    monomial_kernel<<<blocks, threads, 0, st>>>(d_out, t->d_ordinal, t->d_moduli, t->log_n, t->L, coeff, degree, kind);
+    count_launch();
+    PG_LAUNCH_CHECK("monomial_kernel launch");
+    return PG_OK;
+}
+
+static int check_table_data(const pg_ntt_table* t, const void* d, size_t polys) {
+    if (!t) return set_error(PG_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (!d && polys) return set_error(PG_ERR_INVALID_ARGUMENT, "data is NULL");
+    if (t->log_n > 16) return set_error(PG_ERR_UNSUPPORTED, "this build runs NTTs for log_n in [1, 16]");
+    return PG_OK;
+}
+
+static int host_roundtrip(const pg_ntt_table* t, uint64_t* h, size_t polys, int lazy, int mode) {
+    int rc = check_table_data(t, h, polys);
+    if (rc) return rc;
+    if (polys == 0) return PG_OK;
+    const size_t bytes = polys * t->L * t->n * sizeof(uint64_t);
+    uint64_t* d = nullptr;
+    PG_CUDA(cudaMalloc(&d, bytes));
+    cudaError_t e = cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_status(e, "host transform: copy in");
+    }
+    rc = launch_ntt(make_args(t, d, polys * t->L, lazy), t->log_n, mode, 0);
+    if (rc == PG_OK) {
+        e = cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_status(e, "host transform: copy out");
+    }
+    cudaFree(d);
+    return rc;
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+int pg_ntt_forward(const pg_ntt_table* t, uint64_t* d_data, size_t polys, int lazy, void* stream) {
+    int rc = check_table_data(t, d_data, polys);
+    if (rc) return rc;
+    return launch_ntt(make_args(t, d_data, polys * t->L, lazy), t->log_n, MODE_FWD, (cudaStream_t)stream);
+}
+
+int pg_ntt_inverse(const pg_ntt_table* t, uint64_t* d_data, size_t polys, int lazy, void* stream) {
+    int rc = check_table_data(t, d_data, polys);
+    if (rc) return rc;
+    return launch_ntt(make_args(t, d_data, polys * t->L, lazy), t->log_n, MODE_INV, (cudaStream_t)stream);
+}
+
+int pg_ntt_forward_host(const pg_ntt_table* t, uint64_t* h_data, size_t polys, int lazy) {
+    return host_roundtrip(t, h_data, polys, lazy, MODE_FWD);
+}
+
+int pg_ntt_inverse_host(const pg_ntt_table* t, uint64_t* h_data, size_t polys, int lazy) {
+    return host_roundtrip(t, h_data, polys, lazy, MODE_INV);
+}
+
+int pg_ntt_monomial(const pg_ntt_table* t, uint64_t coeff, size_t degree, uint64_t* d_out, void* stream) {
+    return launch_monomial(t, coeff, degree, d_out, 0, (cudaStream_t)stream);
+}
+
+int pg_ntt_coeff_one_monomial(const pg_ntt_table* t, size_t degree, uint64_t* d_out, void* stream) {
+    return launch_monomial(t, 1, degree, d_out, 1, (cudaStream_t)stream);
+}
+
+int pg_ntt_coeff_minus_one_monomial(const pg_ntt_table* t, size_t degree, uint64_t* d_out, void* stream) {
+    return launch_monomial(t, 1, degree, d_out, 2, (cudaStream_t)stream);
+}
+
+int pg_dcrt_polymul_ntt_plain(const pg_ntt_table* t, uint64_t* d_data, const uint64_t* d_plain,
+                              const uint64_t* d_plain_q, size_t polys, void* stream) {
+    int rc = check_table_data(t, d_data, polys);
+    if (rc) return rc;
+    if (!d_plain || !d_plain_q) return set_error(PG_ERR_INVALID_ARGUMENT, "plaintext is NULL");
+    NttArgs a = make_args(t, d_data, polys * t->L, 0);
+    a.plain = d_plain;
+    a.plain_q = d_plain_q;
+    return launch_ntt(a, t->log_n, MODE_RT, (cudaStream_t)stream);
+}
+
+}  // extern "C"

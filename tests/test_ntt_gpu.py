@@ -1,0 +1,193 @@
+"""GPU parity of the NTT family against the oracle (bit-exact, lazy values too).
+
+Covers every supported ring degree (2^1 .. 2^16: single-CTA and cluster
+kernels), single and multi-prime tables, ragged batch counts, the reference's
+input ranges ([0,4q) forward, [0,2q) inverse), host-slice drop-in calls,
+monomial transforms, the fused fwd -> x plain -> inv launch and the golden
+fixtures.  Full-size batches are checked through round-trip identities.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def primes_for(log_n, count, bits=50):
+    return O.ntt_primes(1 << bits, 2 << log_n, count)
+
+
+def lazy_inputs(moduli, n, polys, seed, top):
+    """[polys][L][n] values uniform below top*q_l (top = 4 for forward, 2 for inverse)."""
+    L = len(moduli)
+    out = np.empty((polys, L, n), np.uint64)
+    for p in range(polys):
+        for l, q in enumerate(moduli):
+            out[p, l] = O.uniform(seed, p * L + l, top * q, n)
+    return out
+
+
+@pytest.mark.parametrize("log_n", list(range(1, 17)))
+@pytest.mark.parametrize("L", [1, 3])
+def test_forward_inverse_bit_exact(gpu, log_n, L):
+    n = 1 << log_n
+    moduli = primes_for(log_n, L)
+    polys = 1 if log_n >= 15 else (3 if log_n >= 12 else 5)
+    ref = O.DcrtTable(log_n, moduli)
+    tab = gpu.DcrtTable(log_n, moduli)
+    for lazy in (True, False):
+        x = lazy_inputs(moduli, n, polys, 100 + log_n, 4)
+        buf = gpu.DeviceBuffer.from_numpy(x)
+        tab.forward(buf, polys, lazy=lazy)
+        got = buf.numpy(x.shape)
+        exp = ref.forward(x, lazy=lazy)
+        assert np.array_equal(got, exp.reshape(x.shape)), f"forward lazy={lazy}"
+        y = lazy_inputs(moduli, n, polys, 200 + log_n, 2)
+        buf = gpu.DeviceBuffer.from_numpy(y)
+        tab.inverse(buf, polys, lazy=lazy)
+        got = buf.numpy(y.shape)
+        exp = ref.inverse(y, lazy=lazy)
+        assert np.array_equal(got, exp.reshape(y.shape)), f"inverse lazy={lazy}"
+
+
+@pytest.mark.parametrize("log_n", [1, 4, 9, 10, 12, 13, 14, 16])
+def test_ragged_batches(gpu, log_n):
+    # batch counts that do not fill the last CTA of the multi-row kernels
+    n = 1 << log_n
+    moduli = primes_for(log_n, 2)
+    ref = O.DcrtTable(log_n, moduli)
+    tab = gpu.DcrtTable(log_n, moduli)
+    for polys in ([0, 1, 7, 33, 65] if log_n < 12 else [0, 1, 2]):
+        x = lazy_inputs(moduli, n, max(polys, 1), 7, 4)[:polys].copy()
+        buf = gpu.DeviceBuffer(max(x.size, 1))
+        if polys:
+            buf.upload(x)
+        tab.forward(buf, polys)
+        if polys:
+            assert np.array_equal(buf.numpy()[: x.size].reshape(x.shape), ref.forward(x).reshape(x.shape))
+
+
+@pytest.mark.parametrize("log_n", [1, 5, 10, 11, 13, 14, 15, 16])
+def test_fused_polymul_round_trip(gpu, log_n):
+    n = 1 << log_n
+    L = 3
+    moduli = primes_for(log_n, L)
+    polys = 2
+    ref = O.DcrtTable(log_n, moduli)
+    tab = gpu.DcrtTable(log_n, moduli)
+    x = lazy_inputs(moduli, n, polys, 31, 1)
+    plain = lazy_inputs(moduli, n, 1, 32, 1)[0]
+    exp = ref.polymul_roundtrip(x, plain)
+    buf = gpu.DeviceBuffer.from_numpy(x)
+    pbuf = gpu.DeviceBuffer.from_numpy(plain)
+    qbuf = gpu.DeviceBuffer(plain.size)
+    tab.shoup_prepare(pbuf, qbuf, 1)
+    tab.polymul_ntt_plain(buf, pbuf, qbuf, polys)
+    assert np.array_equal(buf.numpy(x.shape), exp.reshape(x.shape))
+    # and it is the product of the three reference calls
+    b2 = gpu.DeviceBuffer.from_numpy(x)
+    tab.forward(b2, polys)
+    tab.mul(b2, pbuf, polys, rhs_polys=1)
+    tab.inverse(b2, polys)
+    assert np.array_equal(b2.numpy(x.shape), exp.reshape(x.shape))
+
+
+def test_polymul_equals_schoolbook(gpu):
+    # config-1 shape: N = 1024, q = largest prime < 2^50 with q = 1 mod 2048, 64 pairs
+    q = O.ntt_primes(1 << 50, 2048, 1)[0]
+    tab = gpu.NttTable(10, q)
+    a = np.stack([O.uniform(0x5EED0000, 2 * i, q, 1024) for i in range(64)])
+    b = np.stack([O.uniform(0x5EED0000, 2 * i + 1, q, 1024) for i in range(64)])
+    da, db = gpu.DeviceBuffer.from_numpy(a), gpu.DeviceBuffer.from_numpy(b)
+    tab.forward(da, 64)
+    tab.forward(db, 64)
+    tab.mul(da, db, 64)
+    tab.inverse(da, 64)
+    got = da.numpy(a.shape)
+    for i in range(0, 64, 9):
+        assert np.array_equal(got[i], O.naive_negacyclic(a[i], b[i], q))
+
+
+def test_golden_fixtures(gpu):
+    import json
+    arrays = np.load(os.path.join(GOLD, "ntt_golden.npz"))
+    kats = json.load(open(os.path.join(GOLD, "kats.json")))
+    for case in kats["ntt_cases"]:
+        label, log_n, q = case["label"], case["log_n"], case["q"]
+        tab = gpu.NttTable(log_n, q)
+        a = arrays[f"{label}/a"].copy()
+        tab.transform_slice(a)
+        assert np.array_equal(a, arrays[f"{label}/ntt_a"]), label
+        tab.inverse_transform_slice(a)
+        assert np.array_equal(a, arrays[f"{label}/a"]), label
+
+
+def test_host_slice_dropin_lazy(gpu):
+    q = O.ntt_primes(1 << 50, 1 << 12, 1)[0]
+    tab = gpu.NttTable(11, q)
+    ref = O.NttTable(11, q)
+    a = O.uniform(5, 5, 4 * q, 2048)
+    x = a.copy()
+    tab.lazy_transform_slice(x)
+    assert np.array_equal(x, ref.forward(a, lazy=True))
+    y = x % np.uint64(2 * q)
+    z = y.copy()
+    tab.lazy_inverse_transform_slice(z)
+    assert np.array_equal(z, ref.inverse(y, lazy=True))
+    with pytest.raises(ValueError):
+        tab.transform_slice(np.zeros(1000, np.uint64))
+
+
+@pytest.mark.parametrize("log_n", [1, 6, 11, 16])
+def test_monomials(gpu, log_n):
+    n = 1 << log_n
+    moduli = primes_for(log_n, 2)
+    tab = gpu.DcrtTable(log_n, moduli)
+    refs = [O.NttTable(log_n, q) for q in moduli]
+    out = np.zeros(2 * n, np.uint64)
+    for coeff, deg in [(5, min(7, n - 1)), (1, n - 1), (0, 1), (123456789, 0), (moduli[0] - 1, 1)]:
+        tab.transform_monomial(coeff, deg, out)
+        exp = np.concatenate([r.monomial(coeff, deg) for r in refs])
+        assert np.array_equal(out, exp), (coeff, deg)
+    for deg in (0, 1, n - 1):
+        tab.transform_coeff_one_monomial(deg, out)
+        assert np.array_equal(out, np.concatenate([r.coeff_one_monomial(deg) for r in refs]))
+        tab.transform_coeff_minus_one_monomial(deg, out)
+        assert np.array_equal(out, np.concatenate([r.coeff_minus_one_monomial(deg) for r in refs]))
+
+
+def test_extreme_moduli(gpu):
+    # 60-bit HEXL prime (4q < 2^64 still holds) and a tiny prime
+    for log_n, q in [(11, 1152921504606830593), (3, 17), (12, 536813569)]:
+        n = 1 << log_n
+        ref = O.NttTable(log_n, q)
+        tab = gpu.NttTable(log_n, q)
+        a = O.uniform(9, 1, 4 * q, n)
+        buf = gpu.DeviceBuffer.from_numpy(a)
+        tab.forward(buf, 1, lazy=True)
+        assert np.array_equal(buf.numpy(), ref.forward(a, lazy=True))
+
+
+def test_full_size_batched_round_trip(gpu):
+    # the batched workload's shape: N = 2^16, L = 24 primes q = 1 mod 2^17, 128 polys;
+    # fwd -> inv is the identity, and poly 0 equals the oracle bit for bit
+    log_n, L, polys = 16, 24, 128
+    moduli = O.ntt_primes(1 << 50, 1 << 17, L)
+    tab = gpu.DcrtTable(log_n, moduli)
+    buf = gpu.DeviceBuffer(polys * L * (1 << log_n))
+    tab.fill_uniform(buf, polys, seed=0x5EED0001)
+    orig = buf.numpy()
+    tab.forward(buf, polys)
+    fwd = buf.numpy()
+    ref = O.DcrtTable(log_n, moduli)
+    per = L << log_n
+    assert np.array_equal(fwd[:per], ref.forward(orig[:per]))
+    tab.inverse(buf, polys)
+    assert np.array_equal(buf.numpy(), orig)
+    # device generator equals the oracle generator
+    assert np.array_equal(orig[: 1 << log_n], O.uniform(0x5EED0001, 0, moduli[0], 1 << log_n))
