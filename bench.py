@@ -48,6 +48,16 @@ WORKLOAD = {
 ALGO_BYTES = 2 * POLYS * L * N * 8 + L * N * 8
 
 
+def set_polys(p: int):
+    global POLYS, NTT_PER_STEP, ALGO_BYTES
+    if p != POLYS:
+        POLYS = p
+        NTT_PER_STEP = 2 * p
+        ALGO_BYTES = 2 * p * L * N * 8 + L * N * 8
+        WORKLOAD["polys"] = p
+        WORKLOAD["workload"] += f" [reduced to {p} polys for a profiler capture]"
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -331,7 +341,10 @@ def main(argv=None):
     ap.add_argument("--impl", default="primus_b200", choices=["primus_b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--polys", type=int, default=POLYS,
+                    help="polys per step (default 128 = the workload; smaller only for profiler captures)")
     args = ap.parse_args(argv)
+    set_polys(args.polys)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -18,10 +18,44 @@ namespace pg {
 // hi 64 bits of a 64x64 product
 PG_DEV uint64_t mulhi64(uint64_t a, uint64_t b) { return __umul64hi(a, b); }
 
-// Shoup lazy multiply: result in [0, 2q)
-PG_DEV uint64_t shoup_lazy(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {
-    return w * b - q * mulhi64(wq, b);
+// Shoup lazy multiply: result in [0, 2q).  Hand-scheduled in 32-bit pieces:
+// hw = hi64(w' * b) with one carry chain, then w*b - q*hw mod 2^64 computed as
+// w*b + (2^64 - q)*hw with wide multiply-adds (no separate 64-bit subtract).
+// nq = 2^64 - q is passed in precomputed.
+PG_DEV uint64_t shoup_lazy_nq(uint64_t w, uint64_t wq, uint64_t b, uint64_t nq) {
+    uint64_t r;
+    asm("{\n\t"
+        ".reg .u32 a0, a1, b0, b1, t, m0, m1, s0, s1, c2, w0, w1, n0, n1, h0, h1, r0, r1;\n\t"
+        ".reg .u64 m, hw, acc, tz;\n\t"
+        "mov.b64 {a0, a1}, %2;\n\t"
+        "mov.b64 {b0, b1}, %3;\n\t"
+        "mul.hi.u32 t, a0, b0;\n\t"
+        "cvt.u64.u32 tz, t;\n\t"
+        "mad.wide.u32 m, a0, b1, tz;\n\t"
+        "mov.b64 {m0, m1}, m;\n\t"
+        "mad.lo.cc.u32 s0, a1, b0, m0;\n\t"
+        "madc.hi.cc.u32 s1, a1, b0, m1;\n\t"
+        "addc.u32 c2, 0, 0;\n\t"
+        "mov.b64 m, {s1, c2};\n\t"
+        "mad.wide.u32 hw, a1, b1, m;\n\t"
+        "mov.b64 {h0, h1}, hw;\n\t"
+        "mov.b64 {w0, w1}, %1;\n\t"
+        "mov.b64 {n0, n1}, %4;\n\t"
+        "mul.wide.u32 acc, w0, b0;\n\t"
+        "mad.wide.u32 acc, n0, h0, acc;\n\t"
+        "mov.b64 {r0, r1}, acc;\n\t"
+        "mad.lo.u32 r1, w0, b1, r1;\n\t"
+        "mad.lo.u32 r1, w1, b0, r1;\n\t"
+        "mad.lo.u32 r1, n0, h1, r1;\n\t"
+        "mad.lo.u32 r1, n1, h0, r1;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(w), "l"(wq), "l"(b), "l"(nq));
+    return r;
 }
+
+PG_DEV uint64_t shoup_lazy(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) { return shoup_lazy_nq(w, wq, b, 0 - q); }
 
 // Shoup full multiply: result in [0, q)
 PG_DEV uint64_t shoup_mul(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {

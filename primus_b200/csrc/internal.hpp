@@ -85,7 +85,9 @@ struct NttArgs {
     const ulonglong2* inv_last;
     const uint64_t* plain;
     const uint64_t* plain_q;
+    const Barrett* bar;
     uint64_t rows;
+    uint64_t max_modulus;
     uint32_t L;
     int lazy;
 };
@@ -102,7 +104,10 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     a.inv_last = t->d_inv_last;
     a.plain = nullptr;
     a.plain_q = nullptr;
+    a.bar = t->d_barrett;
     a.rows = rows;
+    a.max_modulus = 0;
+    for (uint64_t m : t->moduli) a.max_modulus = m > a.max_modulus ? m : a.max_modulus;
     a.L = t->L;
     a.lazy = lazy;
     return a;

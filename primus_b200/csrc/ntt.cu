@@ -52,28 +52,48 @@ PG_DEV void static_for(F&& f) {
     }
 }
 
-// Harvey forward butterfly; x, y in [0, 4q) -> [0, 4q)
-PG_DEV void fwd_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t q2) {
+// Harvey forward butterfly; x, y in [0, 4q) -> [0, 4q).  nq = 2^64 - q.
+PG_DEV void fwd_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
     uint64_t u = x >= q2 ? x - q2 : x;
-    uint64_t v = shoup_lazy(w.x, w.y, y, q);
+    uint64_t v = shoup_lazy_nq(w.x, w.y, y, nq);
+    x = u + v;
+    y = u + q2 - v;
+}
+
+// Forward butterfly without the u = x mod 2q step.  Used only where the
+// canonical result is returned (transform_slice, the fused round trip): the
+// bound grows by 2q per stage, so after log2(N) <= 16 stages from [0, 4q) the
+// values stay below 36q < 2^64 for q < 2^58, and the final canonical
+// reduction yields the same residues as the Harvey schedule.
+PG_DEV void fwd_bfly_fast(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
+    uint64_t u = x;
+    uint64_t v = shoup_lazy_nq(w.x, w.y, y, nq);
     x = u + v;
     y = u + q2 - v;
 }
 
 // Gentleman-Sande inverse butterfly; x, y in [0, 2q) -> [0, 2q)
-PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t q2) {
+PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
     uint64_t u = x, v = y;
     uint64_t s = u + v;
     x = s >= q2 ? s - q2 : s;
-    y = shoup_lazy(w.x, w.y, u + q2 - v, q);
+    y = shoup_lazy_nq(w.x, w.y, u + q2 - v, nq);
 }
 
 // Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+2q-v), canonical
 PG_DEV void inv_last_bfly(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, uint64_t q,
-                          uint64_t q2) {
+                          uint64_t nq) {
     uint64_t u = x, v = y;
-    x = shoup_mul(s.x, s.y, u + v, q);
-    y = shoup_mul(sr.x, sr.y, u + q2 - v, q);
+    uint64_t a = shoup_lazy_nq(s.x, s.y, u + v, nq);
+    uint64_t b = shoup_lazy_nq(sr.x, sr.y, u + 2 * q - v, nq);
+    x = a >= q ? a - q : a;
+    y = b >= q ? b - q : b;
+}
+
+// any 64-bit v -> v mod q, using floor(2^64/q) (the high word of the Barrett ratio)
+PG_DEV uint64_t reduce_full(uint64_t v, uint64_t q, uint64_t inv64, uint64_t nq) {
+    uint64_t r = v + nq * mulhi64(inv64, v);
+    return r >= q ? r - q : r;
 }
 
 PG_DEV uint64_t canon4(uint64_t v, uint64_t q, uint64_t q2) {
@@ -92,9 +112,9 @@ PG_DEV uint32_t group_base(uint32_t t, int g) {
 // Stage bits P_HI down to P_LO of an M = 2^LOG_M block whose twiddle row base
 // is tw_base (= C + cluster rank; 1 for a whole row): stage bit p uses
 // tw[(tw_base << (LOG_M-1-p)) + (i >> (p+1))].
-template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO>
+template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, bool FAST>
 PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
-                      uint64_t q, uint64_t q2) {
+                      uint64_t q2, uint64_t nq) {
     constexpr int E = 1 << LOG_E;
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
         constexpr int p = P_HI - decltype(it)::value;
@@ -107,7 +127,10 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
             const ulonglong2 w = __ldg(tw + row0 + k);
             static_for<0, half>([&](auto ll) {
                 constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
-                fwd_bfly(x[jj], x[jj + half], w, q, q2);
+                if constexpr (FAST)
+                    fwd_bfly_fast(x[jj], x[jj + half], w, q2, nq);
+                else
+                    fwd_bfly(x[jj], x[jj + half], w, q2, nq);
             });
         });
     });
@@ -119,7 +142,8 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // whole transform (p == LOG_N-1) falls inside the round it is the scaled one.
 template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
-                      ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t q2) {
+                      ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t nq) {
+    const uint64_t q2 = 2 * q;
     constexpr int E = 1 << LOG_E;
     constexpr uint32_t N = 1u << LOG_N;
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
@@ -129,7 +153,7 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
         if constexpr (p == LOG_N - 1) {
             static_for<0, E>([&](auto jt) {
                 constexpr int jj = decltype(jt)::value;
-                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, q2);
+                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq);
             });
         } else {
             const uint32_t row0 = N + 1 - (N >> p) + (((rank << LOG_M) + base) >> (p + 1));
@@ -138,7 +162,7 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
                 const ulonglong2 w = __ldg(itw + row0 + k);
                 static_for<0, half>([&](auto ll) {
                     constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
-                    inv_bfly(x[jj], x[jj + half], w, q, q2);
+                    inv_bfly(x[jj], x[jj + half], w, q2, nq);
                 });
             });
         }
@@ -148,13 +172,16 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
 template <int LOG_E, int G>
 PG_DEV void load_smem(uint64_t (&x)[1 << LOG_E], const uint64_t* sm, uint32_t base) {
 #pragma unroll
-    for (int jj = 0; jj < (1 << LOG_E); ++jj) x[jj] = sm[padi(base + ((uint32_t)jj << G))];
+    // base and jj << G have disjoint bits, so padi(base | off) = padi(base) + padi(off)
+    const uint64_t* p = sm + padi(base);
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) x[jj] = p[padi(jj << G)];
 }
 
 template <int LOG_E, int G>
 PG_DEV void store_smem(const uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t base) {
 #pragma unroll
-    for (int jj = 0; jj < (1 << LOG_E); ++jj) sm[padi(base + ((uint32_t)jj << G))] = x[jj];
+    uint64_t* p = sm + padi(base);
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) p[padi(jj << G)] = x[jj];
 }
 
 // ---- forward rounds 1.. over a block in shared memory (round 0 done by caller)
@@ -170,17 +197,17 @@ struct FwdRounds {
 // Runs forward rounds R..last on x (x holds round R-1's group on entry, which
 // is stored to smem first).  On exit x holds the last round's group (G = 0,
 // i.e. E contiguous elements starting at tid*E).
-template <int LOG_M, int LOG_E, int R>
+template <int LOG_M, int LOG_E, int R, bool FAST>
 PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
-                     const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2) {
+                     const ulonglong2* __restrict__ tw, uint64_t q2, uint64_t nq) {
     using Cur = FwdRounds<LOG_M, LOG_E, R>;
     using Prev = FwdRounds<LOG_M, LOG_E, R - 1>;
     store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
     __syncthreads();
     const uint32_t base = group_base<LOG_E>(tid, Cur::G);
     load_smem<LOG_E, Cur::G>(x, sm, base);
-    fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO>(x, base, tw_base, tw, q, q2);
-    if constexpr (!Cur::LAST) fwd_rest<LOG_M, LOG_E, R + 1>(x, sm, tid, tw_base, tw, q, q2);
+    fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO, FAST>(x, base, tw_base, tw, q2, nq);
+    if constexpr (!Cur::LAST) fwd_rest<LOG_M, LOG_E, R + 1, FAST>(x, sm, tid, tw_base, tw, q2, nq);
 }
 
 template <int LOG_M, int LOG_E, int R>
@@ -195,7 +222,7 @@ struct InvRounds {
 // (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
 template <int LOG_N, int LOG_M, int LOG_E, int R, int R_END>
 PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
-                      const ulonglong2* __restrict__ itw, ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t q2) {
+                      const ulonglong2* __restrict__ itw, ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t nq) {
     if constexpr (R < R_END) {
         using Cur = InvRounds<LOG_M, LOG_E, R>;
         using Prev = InvRounds<LOG_M, LOG_E, R - 1>;
@@ -203,25 +230,31 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
         __syncthreads();
         const uint32_t base = group_base<LOG_E>(tid, Cur::G);
         load_smem<LOG_E, Cur::G>(x, sm, base);
-        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, s, sr, q, q2);
-        inv_range<LOG_N, LOG_M, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, s, sr, q, q2);
+        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, s, sr, q, nq);
+        inv_range<LOG_N, LOG_M, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, s, sr, q, nq);
     }
 }
 
 // ============================================================================
 // Single-CTA kernel: ROWS rows of N = 2^LOG_N per CTA, T = N/E threads per row.
+// FAST selects the forward schedule without per-butterfly reduction of u (only
+// when the caller needs canonical or multiplied outputs and every q < 2^58).
 // ============================================================================
-template <int LOG_N, int LOG_E, int ROWS, int MODE>
+template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
 __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kernel(NttArgs a) {
     constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E;
     extern __shared__ uint64_t smem_block[];
     const uint32_t tid = threadIdx.x;
-    const uint64_t row = (uint64_t)blockIdx.x * ROWS + threadIdx.y;
-    const bool active = row < a.rows;
-    const uint32_t limb = (uint32_t)((active ? row : 0) % a.L);
+    // launch order is limb-major (all polys of limb 0, then limb 1, ...) so that
+    // concurrently running CTAs share one prime's twiddles in L2
+    const uint64_t u = (uint64_t)blockIdx.x * ROWS + threadIdx.y;
+    const bool active = u < a.rows;
+    const uint64_t polys = a.rows / a.L;
+    const uint32_t limb = active ? (uint32_t)(u / polys) : 0;
+    const uint64_t row = active ? (u % polys) * a.L + limb : 0;
     uint64_t* sm = smem_block + threadIdx.y * padded(N);
-    uint64_t* g = a.data + (active ? row : 0) * N;
-    const uint64_t q = a.moduli[limb], q2 = q << 1;
+    uint64_t* g = a.data + row * N;
+    const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
     uint64_t x[E];
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
@@ -230,11 +263,15 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
         // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = active ? g[tid + jj * T] : 0;
-        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO>(x, tid, 1, tw, q, q2);
-        if constexpr (!R0::LAST) fwd_rest<LOG_N, LOG_E, 1>(x, sm, tid, 1, tw, q, q2);
+        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, tw, q2, nq);
+        if constexpr (!R0::LAST) fwd_rest<LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, tw, q2, nq);
         // x = E contiguous outputs at tid*E
         if constexpr (MODE == MODE_FWD) {
-            if (!a.lazy) {
+            if constexpr (FAST) {
+                const uint64_t inv64 = a.bar[limb].r1;
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+            } else if (!a.lazy) {
 #pragma unroll
                 for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
             }
@@ -245,13 +282,13 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
 #pragma unroll
                 for (int k = 0; k < E; ++k) g[tid + k * T] = sm[padi(tid + k * T)];
             }
-            return;
         } else {
-            // pointwise product with the NTT-domain plaintext (Shoup-prepared)
+            // pointwise product with the NTT-domain plaintext (Shoup-prepared);
+            // the lazy product in [0, 2q) is a valid inverse input
             const uint64_t* pv = a.plain + (size_t)limb * N + tid * E;
             const uint64_t* pq = a.plain_q + (size_t)limb * N + tid * E;
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_mul(__ldg(pv + jj), __ldg(pq + jj), canon4(x[jj], q, q2), q);
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
         }
     }
     // ---------------- inverse
@@ -267,13 +304,12 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         } else {
             // round trip: the forward's last group (tid*E .. tid*E+E-1) is the
-            // inverse's first group whenever LOG_N >= LOG_E (I0::G == 0)
+            // inverse's first group (I0::G == 0), so it stays in registers
             static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
-            __syncthreads();  // all forward smem reads done before inverse smem writes
         }
         inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, s, sr, q,
-                                                                  q2);
-        inv_range<LOG_N, LOG_N, LOG_E, 1, (LOG_N + LOG_E - 1) / LOG_E>(x, sm, tid, 0, itw, s, sr, q, q2);
+                                                                  nq);
+        inv_range<LOG_N, LOG_N, LOG_E, 1, (LOG_N + LOG_E - 1) / LOG_E>(x, sm, tid, 0, itw, s, sr, q, nq);
         // last group: elements tid + jj*T, coalesced store
         using Last = InvRounds<LOG_N, LOG_E, (LOG_N + LOG_E - 1) / LOG_E - 1>;
         static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
@@ -302,8 +338,11 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
     asm volatile("st.shared::cluster.u64 [%0], %1;\n" ::"r"(remote), "l"(v) : "memory");
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE>
-__global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttArgs a) {
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
+#ifndef PG_CLUSTER_MIN_BLOCKS
+#define PG_CLUSTER_MIN_BLOCKS 2  // two CTAs per SM: 37 clusters of 8 cover all 148 SMs
+#endif
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) ntt_cluster_kernel(NttArgs a) {
     constexpr int LOG_C = LOG_N - LOG_M;
     constexpr int N = 1 << LOG_N, M = 1 << LOG_M, C = 1 << LOG_C, E = 1 << LOG_E, T = M / E;
     constexpr int K = E / C;       // columns per thread in the cross stages
@@ -313,10 +352,14 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttAr
     uint64_t* sm = smem_cl;
     const uint32_t tid = threadIdx.x;
     const uint32_t rank = blockIdx.x & (C - 1);
-    const uint64_t row = blockIdx.x >> LOG_C;  // grid is exactly rows * C
-    const uint32_t limb = (uint32_t)(row % a.L);
+    // grid is exactly rows * C; clusters run limb-major so that concurrently
+    // running clusters share one prime's twiddles in L2
+    const uint64_t u = blockIdx.x >> LOG_C;
+    const uint64_t polys = a.rows / a.L;
+    const uint32_t limb = (uint32_t)(u / polys);
+    const uint64_t row = (u % polys) * a.L + limb;
     uint64_t* g = a.data + row * N;
-    const uint64_t q = a.moduli[limb], q2 = q << 1;
+    const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
     const uint32_t col0 = rank * SLAB + tid * K;  // first column of this thread
     uint64_t x[E];
 
@@ -339,7 +382,10 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttAr
                     constexpr int k = decltype(kt)::value;
                     static_for<0, half>([&](auto lt) {
                         constexpr int j = (jc << (p + 1)) | decltype(lt)::value;
-                        fwd_bfly(x[k * C + j], x[k * C + j + half], w, q, q2);
+                        if constexpr (FAST)
+                            fwd_bfly_fast(x[k * C + j], x[k * C + j + half], w, q2, nq);
+                        else
+                            fwd_bfly(x[k * C + j], x[k * C + j + half], w, q2, nq);
                     });
                 });
             });
@@ -355,10 +401,15 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttAr
         // local stages: round 0 from smem, then the rest
         using R0 = FwdRounds<LOG_M, LOG_E, 0>;
         load_smem<LOG_E, R0::G>(x, sm, group_base<LOG_E>(tid, R0::G));
-        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO>(x, group_base<LOG_E>(tid, R0::G), C + rank, tw, q, q2);
-        fwd_rest<LOG_M, LOG_E, 1>(x, sm, tid, C + rank, tw, q, q2);
+        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, group_base<LOG_E>(tid, R0::G), C + rank, tw, q2,
+                                                                 nq);
+        fwd_rest<LOG_M, LOG_E, 1, FAST>(x, sm, tid, C + rank, tw, q2, nq);
         if constexpr (MODE == MODE_FWD) {
-            if (!a.lazy) {
+            if constexpr (FAST) {
+                const uint64_t inv64 = a.bar[limb].r1;
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+            } else if (!a.lazy) {
 #pragma unroll
                 for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
             }
@@ -368,89 +419,88 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttAr
             uint64_t* gb = g + rank * M;
 #pragma unroll
             for (int k = 0; k < E; ++k) gb[tid + k * T] = sm[padi(tid + k * T)];
-            return;
         } else {
             const uint64_t* pv = a.plain + (size_t)limb * N + rank * M + tid * E;
             const uint64_t* pq = a.plain_q + (size_t)limb * N + rank * M + tid * E;
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_mul(__ldg(pv + jj), __ldg(pq + jj), canon4(x[jj], q, q2), q);
-            __syncthreads();
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
         }
     }
     // ---------------- inverse
-    if constexpr (MODE == MODE_FWD) return;
-    const ulonglong2* itw = a.inv + (size_t)limb * N;
-    const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
-    using I0 = InvRounds<LOG_M, LOG_E, 0>;
-    if constexpr (MODE == MODE_INV) {
-        uint64_t* gb = g + rank * M;
+    if constexpr (MODE != MODE_FWD) {
+        const ulonglong2* itw = a.inv + (size_t)limb * N;
+        const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
+        using I0 = InvRounds<LOG_M, LOG_E, 0>;
+        if constexpr (MODE == MODE_INV) {
+            uint64_t* gb = g + rank * M;
 #pragma unroll
-        for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = gb[tid + k * T];
-        __syncthreads();
-        load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
-    }
-    inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, s, sr, q,
-                                                              q2);
-    // rounds 1..last: the last round's smem loads are followed by the cluster
-    // arrive so that no CTA overwrites a block another CTA is still reading
-    using ILast = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 1>;
-    static_assert(ILast::G == LOG_M - LOG_E, "last local inverse group");
-    static_assert((LOG_M + LOG_E - 1) / LOG_E >= 2, "cluster path needs two local rounds");
-    inv_range<LOG_N, LOG_M, LOG_E, 1, (LOG_M + LOG_E - 1) / LOG_E - 1>(x, sm, tid, rank, itw, s, sr, q, q2);
-    {
-        using Prev = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 2>;
-        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
-        __syncthreads();
-        const uint32_t base = group_base<LOG_E>(tid, ILast::G);  // == tid
-        load_smem<LOG_E, ILast::G>(x, sm, base);
-        cluster_arrive_relaxed();
-        inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, s, sr, q, q2);
-        cluster_wait_acquire();
-        // element local index tid + jj*T (column c = that index) -> CTA c / SLAB,
-        // column buffer slot [rank][c % SLAB]
-#pragma unroll
-        for (int jj = 0; jj < E; ++jj) {
-            const uint32_t c = tid + jj * T;
-            st_cluster(smem_u32(sm + padi(rank * SLAB + (c & (SLAB - 1)))), c / SLAB, x[jj]);
+            for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = gb[tid + k * T];
+            __syncthreads();
+            load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         }
-        cluster_arrive_release();
-        cluster_wait_acquire();
-    }
-    // cross inverse stages on columns col0 + k: x[k*C + j] = element col0 + k + j*M
+        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, s, sr,
+                                                                  q, nq);
+        // rounds 1..last: the last round's smem loads are followed by the cluster
+        // arrive so that no CTA overwrites a block another CTA is still reading
+        using ILast = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 1>;
+        static_assert(ILast::G == LOG_M - LOG_E, "last local inverse group");
+        static_assert((LOG_M + LOG_E - 1) / LOG_E >= 2, "cluster path needs two local rounds");
+        inv_range<LOG_N, LOG_M, LOG_E, 1, (LOG_M + LOG_E - 1) / LOG_E - 1>(x, sm, tid, rank, itw, s, sr, q, nq);
+        {
+            using Prev = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 2>;
+            store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+            __syncthreads();
+            const uint32_t base = group_base<LOG_E>(tid, ILast::G);  // == tid
+            load_smem<LOG_E, ILast::G>(x, sm, base);
+            cluster_arrive_relaxed();
+            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, s, sr, q, nq);
+            cluster_wait_acquire();
+            // element local index tid + jj*T (column c = that index) -> CTA c / SLAB,
+            // column buffer slot [rank][c % SLAB]
 #pragma unroll
-    for (int k = 0; k < K; ++k)
+            for (int jj = 0; jj < E; ++jj) {
+                const uint32_t c = tid + jj * T;
+                st_cluster(smem_u32(sm + padi(rank * SLAB + (c & (SLAB - 1)))), c / SLAB, x[jj]);
+            }
+            cluster_arrive_release();
+            cluster_wait_acquire();
+        }
+        // cross inverse stages on columns col0 + k: x[k*C + j] = element col0 + k + j*M
 #pragma unroll
-        for (int j = 0; j < C; ++j) x[k * C + j] = sm[padi(j * SLAB + tid * K + k)];
-    static_for<0, LOG_C>([&](auto pt) {
-        constexpr int pp = decltype(pt)::value;  // global stage LOG_M + pp, bit pp of j
-        constexpr int half = 1 << pp;
-        constexpr int stage = LOG_M + pp;
-        if constexpr (stage == LOG_N - 1) {
-            static_for<0, K>([&](auto kt) {
-                constexpr int k = decltype(kt)::value;
-                static_for<0, C>([&](auto jt) {
-                    constexpr int j = decltype(jt)::value;
-                    if constexpr (!(j & half)) inv_last_bfly(x[k * C + j], x[k * C + j + half], s, sr, q, q2);
-                });
-            });
-        } else {
-            static_for<0, (C >> (pp + 1))>([&](auto jt) {
-                constexpr int jc = decltype(jt)::value;
-                const ulonglong2 w = __ldg(itw + (N + 1 - (N >> stage)) + jc);
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < C; ++j) x[k * C + j] = sm[padi(j * SLAB + tid * K + k)];
+        static_for<0, LOG_C>([&](auto pt) {
+            constexpr int pp = decltype(pt)::value;  // global stage LOG_M + pp, bit pp of j
+            constexpr int half = 1 << pp;
+            constexpr int stage = LOG_M + pp;
+            if constexpr (stage == LOG_N - 1) {
                 static_for<0, K>([&](auto kt) {
                     constexpr int k = decltype(kt)::value;
-                    static_for<0, half>([&](auto lt) {
-                        constexpr int j = (jc << (pp + 1)) | decltype(lt)::value;
-                        inv_bfly(x[k * C + j], x[k * C + j + half], w, q, q2);
+                    static_for<0, C>([&](auto jt) {
+                        constexpr int j = decltype(jt)::value;
+                        if constexpr (!(j & half)) inv_last_bfly(x[k * C + j], x[k * C + j + half], s, sr, q, nq);
                     });
                 });
-            });
-        }
-    });
+            } else {
+                static_for<0, (C >> (pp + 1))>([&](auto jt) {
+                    constexpr int jc = decltype(jt)::value;
+                    const ulonglong2 w = __ldg(itw + (N + 1 - (N >> stage)) + jc);
+                    static_for<0, K>([&](auto kt) {
+                        constexpr int k = decltype(kt)::value;
+                        static_for<0, half>([&](auto lt) {
+                            constexpr int j = (jc << (pp + 1)) | decltype(lt)::value;
+                            inv_bfly(x[k * C + j], x[k * C + j + half], w, q2, nq);
+                        });
+                    });
+                });
+            }
+        });
 #pragma unroll
-    for (int k = 0; k < K; ++k)
+        for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int j = 0; j < C; ++j) g[col0 + k + j * M] = x[k * C + j];
+            for (int j = 0; j < C; ++j) g[col0 + k + j * M] = x[k * C + j];
+    }
 }
 
 }  // namespace pg
@@ -460,11 +510,11 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E)) ntt_cluster_kernel(NttAr
 // ============================================================================
 namespace pg {
 
-template <int LOG_N, int LOG_E, int ROWS, int MODE>
+template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
 static int launch_block(const NttArgs& a, cudaStream_t st) {
     constexpr int T = 1 << (LOG_N - LOG_E);
     constexpr size_t smem = (size_t)ROWS * padded(1 << LOG_N) * sizeof(uint64_t);
-    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE>;
+    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE, FAST>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_block_kernel: shared memory attribute");
     dim3 block(T, ROWS);
@@ -475,11 +525,11 @@ static int launch_block(const NttArgs& a, cudaStream_t st) {
     return PG_OK;
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE>
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
 static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
     constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
-    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE>;
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, FAST>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
     if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
@@ -501,35 +551,42 @@ static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     return PG_OK;
 }
 
-template <int MODE>
+template <int MODE, bool FAST>
 static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
     switch (log_n) {
-        case 1: return launch_block<1, 1, 128, MODE>(a, st);
-        case 2: return launch_block<2, 2, 128, MODE>(a, st);
-        case 3: return launch_block<3, 3, 128, MODE>(a, st);
-        case 4: return launch_block<4, 3, 64, MODE>(a, st);
-        case 5: return launch_block<5, 3, 32, MODE>(a, st);
-        case 6: return launch_block<6, 3, 16, MODE>(a, st);
-        case 7: return launch_block<7, 3, 8, MODE>(a, st);
-        case 8: return launch_block<8, 3, 4, MODE>(a, st);
-        case 9: return launch_block<9, 3, 2, MODE>(a, st);
-        case 10: return launch_block<10, 3, 1, MODE>(a, st);
-        case 11: return launch_block<11, 3, 1, MODE>(a, st);
-        case 12: return launch_block<12, 4, 1, MODE>(a, st);
-        case 13: return launch_block<13, 4, 1, MODE>(a, st);
-        case 14: return launch_cluster<14, 13, 4, MODE>(a, st);
-        case 15: return launch_cluster<15, 13, 4, MODE>(a, st);
-        case 16: return launch_cluster<16, 13, 4, MODE>(a, st);
+        case 1: return launch_block<1, 1, 128, MODE, FAST>(a, st);
+        case 2: return launch_block<2, 2, 128, MODE, FAST>(a, st);
+        case 3: return launch_block<3, 3, 128, MODE, FAST>(a, st);
+        case 4: return launch_block<4, 3, 64, MODE, FAST>(a, st);
+        case 5: return launch_block<5, 3, 32, MODE, FAST>(a, st);
+        case 6: return launch_block<6, 3, 16, MODE, FAST>(a, st);
+        case 7: return launch_block<7, 3, 8, MODE, FAST>(a, st);
+        case 8: return launch_block<8, 3, 4, MODE, FAST>(a, st);
+        case 9: return launch_block<9, 3, 2, MODE, FAST>(a, st);
+        case 10: return launch_block<10, 3, 1, MODE, FAST>(a, st);
+        case 11: return launch_block<11, 3, 1, MODE, FAST>(a, st);
+        case 12: return launch_block<12, 4, 1, MODE, FAST>(a, st);
+        case 13: return launch_block<13, 4, 1, MODE, FAST>(a, st);
+        case 14: return launch_cluster<14, 13, 4, MODE, FAST>(a, st);
+        case 15: return launch_cluster<15, 13, 4, MODE, FAST>(a, st);
+        case 16: return launch_cluster<16, 13, 4, MODE, FAST>(a, st);
         default: return set_error(PG_ERR_UNSUPPORTED, "this build runs NTTs for log_n in [1, 16]");
     }
 }
 
+// fast schedule: every modulus below 2^58 so 36q < 2^64 (see fwd_bfly_fast)
+static bool fast_ok(const NttArgs& a) { return a.max_modulus < (1ull << 58); }
+
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
     if (a.rows == 0) return PG_OK;
     switch (mode) {
-        case MODE_FWD: return launch_mode<MODE_FWD>(a, log_n, st);
-        case MODE_INV: return launch_mode<MODE_INV>(a, log_n, st);
-        case MODE_RT: return launch_mode<MODE_RT>(a, log_n, st);
+        case MODE_FWD:
+            if (!a.lazy && fast_ok(a)) return launch_mode<MODE_FWD, true>(a, log_n, st);
+            return launch_mode<MODE_FWD, false>(a, log_n, st);
+        case MODE_INV: return launch_mode<MODE_INV, false>(a, log_n, st);
+        case MODE_RT:
+            if (fast_ok(a)) return launch_mode<MODE_RT, true>(a, log_n, st);
+            return launch_mode<MODE_RT, false>(a, log_n, st);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "bad NTT mode");
 }
