@@ -436,7 +436,10 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
         const HostNttTable& h = t->host[l];
         for (size_t i = 0; i < n; ++i) {
             fwd[l * n + i] = make_ulonglong2(h.root_powers[i], h.root_powers_q[i]);
-            inv[l * n + i] = make_ulonglong2(h.inv_root_powers[i], h.inv_root_powers_q[i]);
+            // device slot j holds inv_root_powers[j + 1] so that pairs used by one
+            // stage start at an even index (32-byte aligned)
+            inv[l * n + i] = i + 1 < n ? make_ulonglong2(h.inv_root_powers[i + 1], h.inv_root_powers_q[i + 1])
+                                       : make_ulonglong2(0, 0);
         }
         for (size_t i = 0; i < 2 * n; ++i) ord[l * 2 * n + i] = make_ulonglong2(h.ordinal[i], h.ordinal_q[i]);
         invn[l] = make_ulonglong2(h.inv_n, h.inv_n_q);

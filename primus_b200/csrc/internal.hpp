@@ -67,7 +67,7 @@ struct pg_ntt_table {
     std::vector<pg::HostNttTable> host;
     uint64_t* d_moduli = nullptr;      // [L]
     ulonglong2* d_fwd = nullptr;       // [L][N] (w, w') bit-reversed root powers
-    ulonglong2* d_inv = nullptr;       // [L][N] (w, w') scrambled inverse powers
+    ulonglong2* d_inv = nullptr;       // [L][N] (w, w') scrambled inverse powers, slot j = index j + 1
     ulonglong2* d_ordinal = nullptr;   // [L][2N] psi^k
     ulonglong2* d_inv_n = nullptr;     // [L] N^-1
     ulonglong2* d_inv_last = nullptr;  // [L] inv_root_powers[N-1] * N^-1

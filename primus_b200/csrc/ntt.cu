@@ -108,10 +108,20 @@ PG_DEV uint32_t group_base(uint32_t t, int g) {
     return ((t >> g) << (g + LOG_E)) | lo;
 }
 
-// One forward round over register group x (x[jj] is local index base + (jj << G)).
-// Stage bits P_HI down to P_LO of an M = 2^LOG_M block whose twiddle row base
-// is tw_base (= C + cluster rank; 1 for a whole row): stage bit p uses
-// tw[(tw_base << (LOG_M-1-p)) + (i >> (p+1))].
+// two consecutive twiddles (value, quotient, value, quotient) with one 256-bit
+// load; p must be 32-byte aligned (callers guarantee an even index)
+PG_DEV void ldg_tw2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
+    uint64_t a0, a1, b0, b1;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a0), "=l"(a1), "=l"(b0), "=l"(b1) : "l"(p));
+    a = make_ulonglong2(a0, a1);
+    b = make_ulonglong2(b0, b1);
+}
+
+// One forward round over register group x (x[jj] is local index base + (jj << G)
+// of a 2^LOG_M block).  Stage bits P_HI down to P_LO; stage bit p is block stage
+// sp = LOG_M-1-p and uses tw[(tw_base << sp) + (i >> (p+1))], tw_base = C + rank
+// for a cluster block (1 for a whole row).  When a stage needs two or more
+// twiddles their first index is even, so they are fetched in 32-byte pairs.
 template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, bool FAST>
 PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
                       uint64_t q2, uint64_t nq) {
@@ -121,10 +131,10 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
         constexpr int r = p - G;
         constexpr int half = 1 << r;
         constexpr int sp = LOG_M - 1 - p;
-        const uint32_t row0 = (tw_base << sp) + (base >> (p + 1));
-        static_for<0, (E >> (r + 1))>([&](auto kk) {
+        constexpr int nk = E >> (r + 1);
+        const ulonglong2* row = tw + (tw_base << sp) + (base >> (p + 1));
+        auto bfly_k = [&](auto kk, const ulonglong2 w) {
             constexpr int k = decltype(kk)::value;
-            const ulonglong2 w = __ldg(tw + row0 + k);
             static_for<0, half>([&](auto ll) {
                 constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
                 if constexpr (FAST)
@@ -132,17 +142,29 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
                 else
                     fwd_bfly(x[jj], x[jj + half], w, q2, nq);
             });
-        });
+        };
+        if constexpr (nk == 1) {
+            bfly_k(IC<0>{}, __ldg(row));
+        } else {
+            static_for<0, nk / 2>([&](auto kp) {
+                constexpr int k = 2 * decltype(kp)::value;
+                ulonglong2 w0, w1;
+                ldg_tw2(row + k, w0, w1);
+                bfly_k(IC<k>{}, w0);
+                bfly_k(IC<k + 1>{}, w1);
+            });
+        }
     });
 }
 
 // One inverse round, stage bits P_LO up to P_HI (gap 2^p).  The element at
-// local index i of CTA rank `rank` has global index rank*M + i; stage p uses
-// inv[N + 1 - (N >> p) + ((rank*M + i) >> (p+1))].  If the last stage of the
-// whole transform (p == LOG_N-1) falls inside the round it is the scaled one.
+// local index i of CTA rank `rank` has row index rank*M + i; stage p uses the
+// inverse powers at N - (N >> p) + ((rank*M + i) >> (p+1)) of the device table,
+// which stores inv_root_powers[j + 1] at j (so paired loads are aligned).  The
+// last stage of the transform (p == LOG_N-1) is the N^-1-scaled one.
 template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
-                      ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t nq) {
+                      const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq) {
     const uint64_t q2 = 2 * q;
     constexpr int E = 1 << LOG_E;
     constexpr uint32_t N = 1u << LOG_N;
@@ -150,88 +172,106 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
         constexpr int p = P_LO + decltype(it)::value;
         constexpr int r = p - G;
         constexpr int half = 1 << r;
+        constexpr int nk = E >> (r + 1);
         if constexpr (p == LOG_N - 1) {
+            const ulonglong2 s = *sptr, sr = *srptr;
             static_for<0, E>([&](auto jt) {
                 constexpr int jj = decltype(jt)::value;
                 if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq);
             });
         } else {
-            const uint32_t row0 = N + 1 - (N >> p) + (((rank << LOG_M) + base) >> (p + 1));
-            static_for<0, (E >> (r + 1))>([&](auto kk) {
+            const ulonglong2* row = itw + (N - (N >> p)) + (((rank << LOG_M) + base) >> (p + 1));
+            auto bfly_k = [&](auto kk, const ulonglong2 w) {
                 constexpr int k = decltype(kk)::value;
-                const ulonglong2 w = __ldg(itw + row0 + k);
                 static_for<0, half>([&](auto ll) {
                     constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
                     inv_bfly(x[jj], x[jj + half], w, q2, nq);
                 });
-            });
+            };
+            if constexpr (nk == 1) {
+                bfly_k(IC<0>{}, __ldg(row));
+            } else {
+                static_for<0, nk / 2>([&](auto kp) {
+                    constexpr int k = 2 * decltype(kp)::value;
+                    ulonglong2 w0, w1;
+                    ldg_tw2(row + k, w0, w1);
+                    bfly_k(IC<k>{}, w0);
+                    bfly_k(IC<k + 1>{}, w1);
+                });
+            }
         }
     });
 }
 
 template <int LOG_E, int G>
 PG_DEV void load_smem(uint64_t (&x)[1 << LOG_E], const uint64_t* sm, uint32_t base) {
-#pragma unroll
     // base and jj << G have disjoint bits, so padi(base | off) = padi(base) + padi(off)
     const uint64_t* p = sm + padi(base);
+#pragma unroll
     for (int jj = 0; jj < (1 << LOG_E); ++jj) x[jj] = p[padi(jj << G)];
 }
 
 template <int LOG_E, int G>
 PG_DEV void store_smem(const uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t base) {
-#pragma unroll
     uint64_t* p = sm + padi(base);
+#pragma unroll
     for (int jj = 0; jj < (1 << LOG_E); ++jj) p[padi(jj << G)] = x[jj];
 }
 
-// ---- forward rounds 1.. over a block in shared memory (round 0 done by caller)
-template <int LOG_M, int LOG_E, int R>
+// Forward rounds over the low TOP bits of a block (the bits above TOP were
+// processed earlier): round R covers bits [P_LO, P_HI], its group spans
+// [P_LO, P_LO + LOG_E).
+template <int TOP, int LOG_E, int R>
 struct FwdRounds {
-    // round R processes bits [P_LO, P_HI]; its group spans [P_LO, P_LO + LOG_E)
-    static constexpr int P_HI = LOG_M - 1 - R * LOG_E;
+    static constexpr int P_HI = TOP - 1 - R * LOG_E;
     static constexpr int P_LO = (P_HI - LOG_E + 1) > 0 ? (P_HI - LOG_E + 1) : 0;
     static constexpr int G = P_LO;
     static constexpr bool LAST = (P_LO == 0);
+    static constexpr int COUNT = (TOP + LOG_E - 1) / LOG_E;
 };
 
-// Runs forward rounds R..last on x (x holds round R-1's group on entry, which
-// is stored to smem first).  On exit x holds the last round's group (G = 0,
-// i.e. E contiguous elements starting at tid*E).
-template <int LOG_M, int LOG_E, int R, bool FAST>
+// Runs forward rounds R..last; x holds round R-1's group on entry (stored to
+// smem first).  On exit x holds the last round's group (G = 0: E contiguous
+// elements at tid*E).
+template <int LOG_M, int TOP, int LOG_E, int R, bool FAST>
 PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
                      const ulonglong2* __restrict__ tw, uint64_t q2, uint64_t nq) {
-    using Cur = FwdRounds<LOG_M, LOG_E, R>;
-    using Prev = FwdRounds<LOG_M, LOG_E, R - 1>;
-    store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
-    __syncthreads();
-    const uint32_t base = group_base<LOG_E>(tid, Cur::G);
-    load_smem<LOG_E, Cur::G>(x, sm, base);
-    fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO, FAST>(x, base, tw_base, tw, q2, nq);
-    if constexpr (!Cur::LAST) fwd_rest<LOG_M, LOG_E, R + 1, FAST>(x, sm, tid, tw_base, tw, q2, nq);
-}
-
-template <int LOG_M, int LOG_E, int R>
-struct InvRounds {
-    static constexpr int P_LO = R * LOG_E;
-    static constexpr int P_HI = (P_LO + LOG_E - 1) < (LOG_M - 1) ? (P_LO + LOG_E - 1) : (LOG_M - 1);
-    static constexpr int G = P_LO < (LOG_M - LOG_E) ? P_LO : (LOG_M - LOG_E);
-    static constexpr bool LAST = (P_HI == LOG_M - 1);
-};
-
-// Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
-// (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
-template <int LOG_N, int LOG_M, int LOG_E, int R, int R_END>
-PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
-                      const ulonglong2* __restrict__ itw, ulonglong2 s, ulonglong2 sr, uint64_t q, uint64_t nq) {
-    if constexpr (R < R_END) {
-        using Cur = InvRounds<LOG_M, LOG_E, R>;
-        using Prev = InvRounds<LOG_M, LOG_E, R - 1>;
+    if constexpr (R < FwdRounds<TOP, LOG_E, 0>::COUNT) {
+        using Cur = FwdRounds<TOP, LOG_E, R>;
+        using Prev = FwdRounds<TOP, LOG_E, R - 1>;
         store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
         __syncthreads();
         const uint32_t base = group_base<LOG_E>(tid, Cur::G);
         load_smem<LOG_E, Cur::G>(x, sm, base);
-        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, s, sr, q, nq);
-        inv_range<LOG_N, LOG_M, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, s, sr, q, nq);
+        fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO, FAST>(x, base, tw_base, tw, q2, nq);
+        fwd_rest<LOG_M, TOP, LOG_E, R + 1, FAST>(x, sm, tid, tw_base, tw, q2, nq);
+    }
+}
+
+template <int TOP, int LOG_E, int R>
+struct InvRounds {
+    static constexpr int P_LO = R * LOG_E;
+    static constexpr int P_HI = (P_LO + LOG_E - 1) < (TOP - 1) ? (P_LO + LOG_E - 1) : (TOP - 1);
+    static constexpr int G = P_LO < (TOP - LOG_E) ? P_LO : (TOP - LOG_E);
+    static constexpr bool LAST = (P_HI == TOP - 1);
+    static constexpr int COUNT = (TOP + LOG_E - 1) / LOG_E;
+};
+
+// Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
+// (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
+template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END>
+PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
+                      const ulonglong2* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
+                      uint64_t nq) {
+    if constexpr (R < R_END) {
+        using Cur = InvRounds<TOP, LOG_E, R>;
+        using Prev = InvRounds<TOP, LOG_E, R - 1>;
+        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+        __syncthreads();
+        const uint32_t base = group_base<LOG_E>(tid, Cur::G);
+        load_smem<LOG_E, Cur::G>(x, sm, base);
+        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, sptr, srptr, q, nq);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, sptr, srptr, q, nq);
     }
 }
 
@@ -264,7 +304,7 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = active ? g[tid + jj * T] : 0;
         fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, tw, q2, nq);
-        if constexpr (!R0::LAST) fwd_rest<LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, tw, q2, nq);
+        fwd_rest<LOG_N, LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, tw, q2, nq);
         // x = E contiguous outputs at tid*E
         if constexpr (MODE == MODE_FWD) {
             if constexpr (FAST) {
@@ -294,7 +334,8 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
         const ulonglong2* itw = a.inv + (size_t)limb * N;
-        const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
+        const ulonglong2* sptr = a.inv_n + limb;
+        const ulonglong2* srptr = a.inv_last + limb;
         using I0 = InvRounds<LOG_N, LOG_E, 0>;
         if constexpr (MODE == MODE_INV) {
             // stage the bit-reversed row through smem (coalesced), then round 0
@@ -307,11 +348,11 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             // inverse's first group (I0::G == 0), so it stays in registers
             static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
         }
-        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, s, sr, q,
-                                                                  nq);
-        inv_range<LOG_N, LOG_N, LOG_E, 1, (LOG_N + LOG_E - 1) / LOG_E>(x, sm, tid, 0, itw, s, sr, q, nq);
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr, srptr,
+                                                                  q, nq);
+        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT>(x, sm, tid, 0, itw, sptr, srptr, q, nq);
         // last group: elements tid + jj*T, coalesced store
-        using Last = InvRounds<LOG_N, LOG_E, (LOG_N + LOG_E - 1) / LOG_E - 1>;
+        using Last = InvRounds<LOG_N, LOG_E, I0::COUNT - 1>;
         static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
         if (active) {
 #pragma unroll
@@ -322,8 +363,13 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
 
 // ============================================================================
 // Cluster kernel: a row of N = 2^LOG_N is owned by C = 2^(LOG_N - LOG_M) CTAs.
-// CTA `rank` owns the contiguous block [rank*M, (rank+1)*M) for the local
-// stages and the column slab [rank*M/C, (rank+1)*M/C) for the cross stages.
+//   cross phase: thread gt = rank*T + tid owns the column {gt + jj*N/E} (the
+//     top LOG_E index bits vary), i.e. the first LOG_E forward stages (last
+//     LOG_E inverse stages); coalesced HBM access.
+//   local phase: CTA rank owns block [rank*M, (rank+1)*M) in shared memory and
+//     runs the remaining stages in rounds of LOG_E.
+// The two phases exchange through distributed shared memory
+// (st.shared::cluster) between cluster barriers.
 // ============================================================================
 PG_DEV void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
 PG_DEV void cluster_arrive_release() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
@@ -338,20 +384,22 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
     asm volatile("st.shared::cluster.u64 [%0], %1;\n" ::"r"(remote), "l"(v) : "memory");
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
 #ifndef PG_CLUSTER_MIN_BLOCKS
 #define PG_CLUSTER_MIN_BLOCKS 2  // two CTAs per SM: 37 clusters of 8 cover all 148 SMs
 #endif
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
 __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) ntt_cluster_kernel(NttArgs a) {
     constexpr int LOG_C = LOG_N - LOG_M;
-    constexpr int N = 1 << LOG_N, M = 1 << LOG_M, C = 1 << LOG_C, E = 1 << LOG_E, T = M / E;
-    constexpr int K = E / C;       // columns per thread in the cross stages
-    constexpr int SLAB = M / C;    // columns per CTA
-    static_assert(K >= 1 && K * T == SLAB, "column split");
+    constexpr int N = 1 << LOG_N, M = 1 << LOG_M, E = 1 << LOG_E, LOG_T = LOG_M - LOG_E, T = 1 << LOG_T;
+    constexpr int LOG_K = LOG_E - LOG_C;  // top block bits handled by the cross phase
+    constexpr int K = 1 << LOG_K;
+    constexpr int TOP = LOG_M - LOG_K;    // block bits handled by the local rounds
+    constexpr int GX = LOG_N - LOG_E;     // cross group stride bit (N/E)
+    static_assert(LOG_K >= 0 && TOP >= LOG_E, "shape");
     extern __shared__ uint64_t smem_cl[];
     uint64_t* sm = smem_cl;
     const uint32_t tid = threadIdx.x;
-    const uint32_t rank = blockIdx.x & (C - 1);
+    const uint32_t rank = blockIdx.x & ((1 << LOG_C) - 1);
     // grid is exactly rows * C; clusters run limb-major so that concurrently
     // running clusters share one prime's twiddles in L2
     const uint64_t u = blockIdx.x >> LOG_C;
@@ -359,51 +407,31 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) n
     const uint32_t limb = (uint32_t)(u / polys);
     const uint64_t row = (u % polys) * a.L + limb;
     uint64_t* g = a.data + row * N;
-    const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
-    const uint32_t col0 = rank * SLAB + tid * K;  // first column of this thread
+    const uint64_t q = a.moduli[limb], nq = 0 - q;
+    const uint32_t gt = (rank << LOG_T) + tid;  // cross group (column) of this thread
     uint64_t x[E];
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+        const uint64_t q2 = q << 1;
         const ulonglong2* tw = a.fwd + (size_t)limb * N;
         cluster_arrive_relaxed();  // matched by the wait before the first remote store
-        // cross stages on columns: x[k*C + j] = row[col0 + k + j*M]
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int j = 0; j < C; ++j) x[k * C + j] = g[col0 + k + j * M];
-        static_for<0, LOG_C>([&](auto st) {
-            constexpr int stg = decltype(st)::value;
-            constexpr int p = LOG_C - 1 - stg;  // bit of j
-            constexpr int half = 1 << p;
-            static_for<0, (C >> (p + 1))>([&](auto jt) {
-                constexpr int jc = decltype(jt)::value;
-                const ulonglong2 w = __ldg(tw + (1 << stg) + jc);
-                static_for<0, K>([&](auto kt) {
-                    constexpr int k = decltype(kt)::value;
-                    static_for<0, half>([&](auto lt) {
-                        constexpr int j = (jc << (p + 1)) | decltype(lt)::value;
-                        if constexpr (FAST)
-                            fwd_bfly_fast(x[k * C + j], x[k * C + j + half], w, q2, nq);
-                        else
-                            fwd_bfly(x[k * C + j], x[k * C + j + half], w, q2, nq);
-                    });
-                });
-            });
-        });
+        for (int jj = 0; jj < E; ++jj) x[jj] = g[gt + (jj << GX)];
+        fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, FAST>(x, gt, 1, tw, q2, nq);
         cluster_wait_acquire();  // every CTA of the cluster is running
-        // scatter: element (column c, j) -> CTA j, local index c
+        // element gt + jj*N/E lives in block jj >> LOG_K at local index gt + (jj & (K-1)) * N/E
+        const uint32_t la = smem_u32(sm + padi(gt));
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int j = 0; j < C; ++j) st_cluster(smem_u32(sm + padi(col0 + k)), j, x[k * C + j]);
+        for (int jj = 0; jj < E; ++jj)
+            st_cluster(la + 8 * padi((jj & (K - 1)) << GX), (uint32_t)(jj >> LOG_K), x[jj]);
         cluster_arrive_release();
         cluster_wait_acquire();
-        // local stages: round 0 from smem, then the rest
-        using R0 = FwdRounds<LOG_M, LOG_E, 0>;
+        // local rounds over the low TOP block bits
+        using R0 = FwdRounds<TOP, LOG_E, 0>;
         load_smem<LOG_E, R0::G>(x, sm, group_base<LOG_E>(tid, R0::G));
-        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, group_base<LOG_E>(tid, R0::G), C + rank, tw, q2,
-                                                                 nq);
-        fwd_rest<LOG_M, LOG_E, 1, FAST>(x, sm, tid, C + rank, tw, q2, nq);
+        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, group_base<LOG_E>(tid, R0::G), (1u << LOG_C) + rank,
+                                                                 tw, q2, nq);
+        fwd_rest<LOG_M, TOP, LOG_E, 1, FAST>(x, sm, tid, (1u << LOG_C) + rank, tw, q2, nq);
         if constexpr (MODE == MODE_FWD) {
             if constexpr (FAST) {
                 const uint64_t inv64 = a.bar[limb].r1;
@@ -429,8 +457,9 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) n
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
         const ulonglong2* itw = a.inv + (size_t)limb * N;
-        const ulonglong2 s = a.inv_n[limb], sr = a.inv_last[limb];
-        using I0 = InvRounds<LOG_M, LOG_E, 0>;
+        using I0 = InvRounds<TOP, LOG_E, 0>;
+        using ILast = InvRounds<TOP, LOG_E, I0::COUNT - 1>;
+        static_assert(I0::COUNT >= 2, "cluster path needs two local rounds");
         if constexpr (MODE == MODE_INV) {
             uint64_t* gb = g + rank * M;
 #pragma unroll
@@ -438,68 +467,40 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) n
             __syncthreads();
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         }
-        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, s, sr,
-                                                                  q, nq);
-        // rounds 1..last: the last round's smem loads are followed by the cluster
-        // arrive so that no CTA overwrites a block another CTA is still reading
-        using ILast = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 1>;
-        static_assert(ILast::G == LOG_M - LOG_E, "last local inverse group");
-        static_assert((LOG_M + LOG_E - 1) / LOG_E >= 2, "cluster path needs two local rounds");
-        inv_range<LOG_N, LOG_M, LOG_E, 1, (LOG_M + LOG_E - 1) / LOG_E - 1>(x, sm, tid, rank, itw, s, sr, q, nq);
+        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, nullptr,
+                                                                  nullptr, q, nq);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1>(x, sm, tid, rank, itw, nullptr, nullptr, q, nq);
         {
-            using Prev = InvRounds<LOG_M, LOG_E, (LOG_M + LOG_E - 1) / LOG_E - 2>;
+            // last local round: its smem loads precede the cluster arrive, so no
+            // CTA overwrites a block that another CTA is still reading
+            using Prev = InvRounds<TOP, LOG_E, I0::COUNT - 2>;
             store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
             __syncthreads();
-            const uint32_t base = group_base<LOG_E>(tid, ILast::G);  // == tid
+            const uint32_t base = group_base<LOG_E>(tid, ILast::G);
             load_smem<LOG_E, ILast::G>(x, sm, base);
             cluster_arrive_relaxed();
-            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, s, sr, q, nq);
+            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, nullptr, nullptr, q,
+                                                                               nq);
             cluster_wait_acquire();
-            // element local index tid + jj*T (column c = that index) -> CTA c / SLAB,
-            // column buffer slot [rank][c % SLAB]
+            // element at row index i = rank*M + base + (jj << G) belongs to cross
+            // group c = i mod N/E (CTA c >> LOG_T, thread c mod T) as element i >> GX:
+            // it goes to slot (i >> GX) * T + (c mod T) of that CTA's buffer
+            const uint32_t i0 = (rank << LOG_M) + base;
 #pragma unroll
             for (int jj = 0; jj < E; ++jj) {
-                const uint32_t c = tid + jj * T;
-                st_cluster(smem_u32(sm + padi(rank * SLAB + (c & (SLAB - 1)))), c / SLAB, x[jj]);
+                const uint32_t i = i0 + ((uint32_t)jj << ILast::G);
+                const uint32_t c = i & ((1u << GX) - 1);
+                st_cluster(smem_u32(sm + padi(((i >> GX) << LOG_T) + (c & (T - 1)))), c >> LOG_T, x[jj]);
             }
             cluster_arrive_release();
             cluster_wait_acquire();
         }
-        // cross inverse stages on columns col0 + k: x[k*C + j] = element col0 + k + j*M
+        // cross inverse stages (the last LOG_E, including the N^-1-scaled one)
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int jj = 0; jj < E; ++jj) x[jj] = sm[padi((jj << LOG_T) + tid)];
+        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1>(x, gt, 0, itw, a.inv_n + limb, a.inv_last + limb, q, nq);
 #pragma unroll
-            for (int j = 0; j < C; ++j) x[k * C + j] = sm[padi(j * SLAB + tid * K + k)];
-        static_for<0, LOG_C>([&](auto pt) {
-            constexpr int pp = decltype(pt)::value;  // global stage LOG_M + pp, bit pp of j
-            constexpr int half = 1 << pp;
-            constexpr int stage = LOG_M + pp;
-            if constexpr (stage == LOG_N - 1) {
-                static_for<0, K>([&](auto kt) {
-                    constexpr int k = decltype(kt)::value;
-                    static_for<0, C>([&](auto jt) {
-                        constexpr int j = decltype(jt)::value;
-                        if constexpr (!(j & half)) inv_last_bfly(x[k * C + j], x[k * C + j + half], s, sr, q, nq);
-                    });
-                });
-            } else {
-                static_for<0, (C >> (pp + 1))>([&](auto jt) {
-                    constexpr int jc = decltype(jt)::value;
-                    const ulonglong2 w = __ldg(itw + (N + 1 - (N >> stage)) + jc);
-                    static_for<0, K>([&](auto kt) {
-                        constexpr int k = decltype(kt)::value;
-                        static_for<0, half>([&](auto lt) {
-                            constexpr int j = (jc << (pp + 1)) | decltype(lt)::value;
-                            inv_bfly(x[k * C + j], x[k * C + j + half], w, q2, nq);
-                        });
-                    });
-                });
-            }
-        });
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int j = 0; j < C; ++j) g[col0 + k + j * M] = x[k * C + j];
+        for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
     }
 }
 
