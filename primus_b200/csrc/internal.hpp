@@ -8,7 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/primus_gpu.h"
+#include "primus_gpu.h"
 #include "common.cuh"
 
 namespace pg {

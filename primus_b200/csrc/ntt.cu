@@ -384,11 +384,15 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
     asm volatile("st.shared::cluster.u64 [%0], %1;\n" ::"r"(remote), "l"(v) : "memory");
 }
 
-#ifndef PG_CLUSTER_MIN_BLOCKS
-#define PG_CLUSTER_MIN_BLOCKS 2  // two CTAs per SM: 37 clusters of 8 cover all 148 SMs
-#endif
+// CTAs per SM the register budget is sized for: the whole 64K-entry register
+// file is shared by MINB CTAs of T threads, i.e. 65536 / (MINB * T) registers
+// per thread (64 for the shapes below), so independent CTAs overlap each
+// other's barrier and exchange phases.
+__host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
+
 template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
-__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) ntt_cluster_kernel(NttArgs a) {
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
+    ntt_cluster_kernel(NttArgs a) {
     constexpr int LOG_C = LOG_N - LOG_M;
     constexpr int N = 1 << LOG_N, M = 1 << LOG_M, E = 1 << LOG_E, LOG_T = LOG_M - LOG_E, T = 1 << LOG_T;
     constexpr int LOG_K = LOG_E - LOG_C;  // top block bits handled by the cross phase
@@ -414,7 +418,9 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) n
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
         const uint64_t q2 = q << 1;
         const ulonglong2* tw = a.fwd + (size_t)limb * N;
-        cluster_arrive_relaxed();  // matched by the wait before the first remote store
+        // matched by the wait before the first remote store; relaxed is enough
+        // because this CTA has not touched shared memory yet
+        cluster_arrive_relaxed();
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = g[gt + (jj << GX)];
         fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, FAST>(x, gt, 1, tw, q2, nq);
@@ -478,7 +484,9 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), PG_CLUSTER_MIN_BLOCKS) n
             __syncthreads();
             const uint32_t base = group_base<LOG_E>(tid, ILast::G);
             load_smem<LOG_E, ILast::G>(x, sm, base);
-            cluster_arrive_relaxed();
+            // release: these shared-memory reads must be performed before any
+            // other CTA, released by this barrier, overwrites the block
+            cluster_arrive_release();
             inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, nullptr, nullptr, q,
                                                                                nq);
             cluster_wait_acquire();
@@ -546,11 +554,20 @@ static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
+    if constexpr (C > 8) {
+        static const cudaError_t np = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (np != cudaSuccess) return cuda_status(np, "ntt_cluster_kernel: non-portable cluster size");
+    }
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
     count_launch();
     if (e != cudaSuccess) return cuda_status(e, "ntt_cluster_kernel launch");
     return PG_OK;
 }
+
+// block size (2^PG_NTT_LOG_M elements) each CTA of a cluster owns
+#ifndef PG_NTT_LOG_M
+#define PG_NTT_LOG_M 12
+#endif
 
 template <int MODE, bool FAST>
 static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
@@ -568,9 +585,9 @@ static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
         case 11: return launch_block<11, 3, 1, MODE, FAST>(a, st);
         case 12: return launch_block<12, 4, 1, MODE, FAST>(a, st);
         case 13: return launch_block<13, 4, 1, MODE, FAST>(a, st);
-        case 14: return launch_cluster<14, 13, 4, MODE, FAST>(a, st);
-        case 15: return launch_cluster<15, 13, 4, MODE, FAST>(a, st);
-        case 16: return launch_cluster<16, 13, 4, MODE, FAST>(a, st);
+        case 14: return launch_cluster<14, PG_NTT_LOG_M, 4, MODE, FAST>(a, st);
+        case 15: return launch_cluster<15, PG_NTT_LOG_M, 4, MODE, FAST>(a, st);
+        case 16: return launch_cluster<16, PG_NTT_LOG_M, 4, MODE, FAST>(a, st);
         default: return set_error(PG_ERR_UNSUPPORTED, "this build runs NTTs for log_n in [1, 16]");
     }
 }

@@ -175,19 +175,52 @@ def test_extreme_moduli(gpu):
 
 def test_full_size_batched_round_trip(gpu):
     # the batched workload's shape: N = 2^16, L = 24 primes q = 1 mod 2^17, 128 polys;
-    # fwd -> inv is the identity, and poly 0 equals the oracle bit for bit
+    # fwd -> inv is the identity on every row, repeated so that an ordering race
+    # between the cluster CTAs' shared-memory exchange would show up; poly 0 and
+    # poly 127 equal the oracle bit for bit
     log_n, L, polys = 16, 24, 128
     moduli = O.ntt_primes(1 << 50, 1 << 17, L)
     tab = gpu.DcrtTable(log_n, moduli)
     buf = gpu.DeviceBuffer(polys * L * (1 << log_n))
     tab.fill_uniform(buf, polys, seed=0x5EED0001)
     orig = buf.numpy()
-    tab.forward(buf, polys)
-    fwd = buf.numpy()
     ref = O.DcrtTable(log_n, moduli)
     per = L << log_n
-    assert np.array_equal(fwd[:per], ref.forward(orig[:per]))
-    tab.inverse(buf, polys)
-    assert np.array_equal(buf.numpy(), orig)
+    for rep in range(3):
+        tab.forward(buf, polys)
+        if rep == 0:
+            fwd = buf.numpy()
+            assert np.array_equal(fwd[:per], ref.forward(orig[:per], threads=8))
+            assert np.array_equal(fwd[-per:], ref.forward(orig[-per:], threads=8))
+        tab.inverse(buf, polys)
+        got = buf.numpy()
+        bad = np.nonzero((got != orig).reshape(polys * L, -1).any(axis=1))[0]
+        assert bad.size == 0, f"rep {rep}: rows {bad[:8].tolist()} differ"
     # device generator equals the oracle generator
     assert np.array_equal(orig[: 1 << log_n], O.uniform(0x5EED0001, 0, moduli[0], 1 << log_n))
+
+
+def test_full_size_fused_round_trip_repeatable(gpu):
+    # fused fwd -> x plain -> inv at full size: poly 0 equals the oracle and the
+    # whole batch is identical across repeated launches (no exchange races)
+    log_n, L, polys = 16, 24, 128
+    moduli = O.ntt_primes(1 << 50, 1 << 17, L)
+    tab = gpu.DcrtTable(log_n, moduli)
+    src = gpu.DeviceBuffer(polys * L * (1 << log_n))
+    tab.fill_uniform(src, polys, seed=0x5EED0002)
+    x = src.numpy()
+    plain = O.uniform_rns(0x5EED0003, 0, moduli, 1 << log_n)
+    pb, qb = gpu.DeviceBuffer.from_numpy(plain), gpu.DeviceBuffer(plain.size)
+    tab.shoup_prepare(pb, qb, 1)
+    first = None
+    for rep in range(3):
+        buf = gpu.DeviceBuffer.from_numpy(x)
+        tab.polymul_ntt_plain(buf, pb, qb, polys)
+        got = buf.numpy()
+        if first is None:
+            first = got
+            per = L << log_n
+            exp = O.DcrtTable(log_n, moduli).polymul_roundtrip(x[:per], plain, threads=8)
+            assert np.array_equal(got[:per], exp)
+        else:
+            assert np.array_equal(got, first), f"rep {rep} differs"
