@@ -190,6 +190,100 @@ int pg_dcrt_polymul_ntt_plain(const pg_ntt_table *table, uint64_t *d_data,
                               const uint64_t *d_plain, const uint64_t *d_plain_q, size_t polys,
                               void *stream);
 
+/* ------------------------------------------------------------- RNS base
+ * RNSBase (primus_rns/src/base.rs:24-90): moduli, Q = prod q_i as a BigUint of
+ * W little-endian limbs, punctured products Q/q_i and their inverses mod q_i.
+ * Fails with PG_ERR_NOT_COPRIME like RNSBase::new. */
+typedef struct pg_rns_base pg_rns_base;
+
+int pg_rns_base_create(const uint64_t *h_moduli, uint32_t moduli_count, pg_rns_base **out);
+int pg_rns_base_destroy(pg_rns_base *base);
+/* moduli_count(), big_uint_value_len() (= W); h_product receives W limbs if non-NULL */
+int pg_rns_base_info(const pg_rns_base *base, uint32_t *moduli_count, uint32_t *big_uint_len,
+                     uint64_t *h_product);
+/* CRT composition of `count` values: residues [L][count] -> BigUint [count][W]
+ * in [0, Q) (compose_multiple_values_inplace, base.rs:422-449) */
+int pg_rns_compose(const pg_rns_base *base, const uint64_t *d_residues, uint64_t *d_values,
+                   size_t count, void *stream);
+/* BigUint [count][W] -> residues [L][count] (decompose_big_uint_values_inplace,
+ * base.rs:285-309) */
+int pg_rns_decompose(const pg_rns_base *base, const uint64_t *d_values, uint64_t *d_residues,
+                     size_t count, void *stream);
+/* signed lift of small values in [0, small_modulus) into every residue
+ * (wrapping_decompose_small_values_inplace, base.rs:201-231) */
+int pg_rns_wrapping_decompose_small(const pg_rns_base *base, const uint64_t *d_small,
+                                    uint64_t *d_residues, size_t count, uint64_t small_modulus,
+                                    void *stream);
+
+/* ------------------------------------------------------ fast base conversion
+ * BaseConverter (primus_rns/src/converter.rs:12-47); fast_convert_array
+ * (:147-175): y_j = sum_i [x_i * (Q/q_i)^-1]_{q_i} * (Q/q_i mod p_j) mod p_j,
+ * no correction, input [L_in][n] -> output [L_out][n]. */
+typedef struct pg_base_converter pg_base_converter;
+
+int pg_base_converter_create(const pg_rns_base *ibase, const pg_rns_base *obase,
+                             pg_base_converter **out);
+int pg_base_converter_destroy(pg_base_converter *conv);
+int pg_fast_convert_array(const pg_base_converter *conv, const uint64_t *d_in, uint64_t *d_out,
+                          size_t n, void *stream);
+
+/* ----------------------------------------------------- gadget decomposition
+ * BigUintApproxSignedBasis (primus_decompose/src/big_integer/basis.rs:34-193)
+ * over the product of an RNS base; reverse_length < 0 means None. */
+typedef struct pg_gadget_basis pg_gadget_basis;
+
+int pg_gadget_basis_create(const pg_rns_base *base, uint32_t log_basis, int32_t reverse_length,
+                           pg_gadget_basis **out);
+int pg_gadget_basis_destroy(pg_gadget_basis *basis);
+/* decompose_length(), drop_bits(), and the gadget scalars' residues [d][L] */
+int pg_gadget_basis_info(const pg_gadget_basis *basis, uint32_t *decompose_length,
+                         uint32_t *drop_bits, uint64_t *h_scalar_residues);
+/* every unsigned digit of `count` BigUint values [count][W] -> [d][count],
+ * digits in [0, B): init_value_carry_slice (basis.rs:307-342) then
+ * unsigned_decompose_slice_inplace per level (common.rs:184-200) */
+int pg_gadget_decompose(const pg_gadget_basis *basis, const uint64_t *d_values,
+                        uint64_t *d_digits, size_t count, void *stream);
+/* the same digits lifted into the RNS base: [d][L][count]
+ * (wrapping_decompose_small_values_inplace applied per level) */
+int pg_gadget_decompose_lift(const pg_gadget_basis *basis, const uint64_t *d_values,
+                             uint64_t *d_residues, size_t count, void *stream);
+
+/* --------------------------------------------- GLev MAC, external product, key switch
+ * Layouts: GLWE = (k+1) DCRT polys [a_1..a_k, b] (primus_lattice/src/glwe/dcrt.rs:19-27);
+ * GLev = d GLWEs (glev/dcrt.rs:16-24); GGSW = (k+1) GLevs (ggsw/dcrt.rs:10-21).
+ * Key and GGSW operands are in the NTT domain; outputs are canonical NTT-domain
+ * residues.  The table's moduli must equal the basis's RNS base.  Scratch:
+ * pass d_workspace of at least *_workspace_size() bytes, or NULL to let the
+ * call take stream-ordered scratch (cudaMallocAsync) and release it. */
+/* batch GLWE (CRT/coefficient form, [batch][k+1][L][N]) x one GGSW -> GLWE
+ * (NTT domain, [batch][k+1][L][N]); CrtGlwe::mul_dcrt_ggsw_inplace
+ * (primus_lattice/src/glwe/crt.rs:202-229) */
+size_t pg_ext_product_workspace_size(const pg_ntt_table *table, const pg_gadget_basis *basis,
+                                     uint32_t k, size_t batch);
+int pg_ext_product(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                   const uint64_t *d_glwe_in, const uint64_t *d_ggsw, uint64_t *d_glwe_out,
+                   size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
+/* acc ([k+1][L][N], NTT domain) += GLev x poly, the poly as CRT residues [L][N]
+ * (add_dcrt_glev_mul_crt_poly_assign, glwe/dcrt.rs:170-247) or as BigUints
+ * [N][W] (add_dcrt_glev_mul_big_uint_poly_assign, glwe/dcrt.rs:249-325) */
+int pg_glev_mac_crt_poly(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                         uint64_t *d_acc, const uint64_t *d_glev, const uint64_t *d_crt_poly,
+                         void *d_workspace, size_t workspace_bytes, void *stream);
+int pg_glev_mac_big_uint_poly(const pg_ntt_table *table, const pg_gadget_basis *basis,
+                              uint32_t k, uint64_t *d_acc, const uint64_t *d_glev,
+                              const uint64_t *d_big_poly, void *d_workspace,
+                              size_t workspace_bytes, void *stream);
+/* key switch s_in -> s_out of a batch: key [k_in][d][k_out+1][L][N] (NTT),
+ * c_in [batch][k_in+1][L][N] (coefficient form), c_out [batch][k_out+1][L][N]
+ * (NTT domain); CrtGlweKeySwitchingKey::key_swithching_inplace
+ * (primus_fhe_core/src/key_switch.rs:79-128) */
+size_t pg_key_switch_workspace_size(const pg_ntt_table *table, const pg_gadget_basis *basis,
+                                    uint32_t k_in, uint32_t k_out, size_t batch);
+int pg_key_switch(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k_in,
+                  uint32_t k_out, const uint64_t *d_key, const uint64_t *d_c_in,
+                  uint64_t *d_c_out, size_t batch, void *d_workspace, size_t workspace_bytes,
+                  void *stream);
+
 /* ------------------------------------------------------- seeded inputs
  * Device-side fill with the counter-based generator (uniform below q_l per
  * limb; stream id = stream0 + poly*L + limb). */

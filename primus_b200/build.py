@@ -4,7 +4,7 @@ Compiles every primus_b200/csrc/*.cu with nvcc for `sm_100a` (one object per
 translation unit, in parallel) and links them into primus_b200/libprimus_gpu.so.
 The CUDA runtime is linked statically, so the library only needs the driver.
 
-    python -m primus_b200.build [--force] [--jobs N]
+    python primus_b200/build.py [--force] [--jobs N]
 """
 from __future__ import annotations
 

@@ -1,0 +1,285 @@
+// GLev multiply-accumulate, GLWE x GGSW external product and RNS key switch.
+//
+//   DcrtGlwe::add_dcrt_glev_mul_crt_poly_assign     primus_lattice/src/glwe/dcrt.rs:170-247
+//   DcrtGlwe::add_dcrt_glev_mul_big_uint_poly_assign primus_lattice/src/glwe/dcrt.rs:249-325
+//   CrtGlwe::mul_dcrt_ggsw_inplace                  primus_lattice/src/glwe/crt.rs:202-229
+//   CrtGlweKeySwitchingKey::key_swithching_inplace  primus_fhe_core/src/key_switch.rs:79-128
+//
+// Layouts (all uint64, limb-major polys [L][N]):
+//   GLWE  = (k+1) polys [a_1 .. a_k, b]             (glwe/dcrt.rs:19-27)
+//   GLev  = d GLWEs, one per gadget digit            (glev/dcrt.rs:16-24)
+//   GGSW  = (k+1) GLevs, one per input component     (ggsw/dcrt.rs:10-21)
+//   key-switching key = k_in GLevs over k_out+1 output polys (key_switch.rs:17-24)
+//
+// Batched pipeline (one launch per step for the whole batch): CRT compose of
+// every input poly -> signed gadget digits lifted into the RNS base -> forward
+// NTT of every digit row -> one multiply-accumulate kernel that forms every
+// output coefficient as sum_{i,j} key[i][j][c] * digit[i][j] with a 128-bit
+// accumulator.  Outputs are canonical NTT-domain residues, equal to the
+// reference's sequential per-digit MAC.
+#include <algorithm>
+
+#include "internal.hpp"
+
+namespace pg {
+uint32_t rns_L(const pg_rns_base* b);
+uint32_t rns_W(const pg_rns_base* b);
+const uint64_t* rns_moduli(const pg_rns_base* b);
+const pg_rns_base* gadget_base(const pg_gadget_basis* g);
+uint32_t gadget_d(const pg_gadget_basis* g);
+int launch_compose(const pg_rns_base* b, const uint64_t* res, uint64_t* out, size_t count, size_t n, uint32_t ppg,
+                   size_t group_stride, cudaStream_t st);
+int launch_gadget(const pg_gadget_basis* g, const uint64_t* vals, uint64_t* out, size_t count, size_t n, bool lift,
+                  cudaStream_t st);
+}  // namespace pg
+
+using namespace pg;
+
+namespace {
+
+PG_DEV void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, uint64_t b) {
+    uint64_t pl = a * b, ph = mulhi64(a, b);
+    lo += pl;
+    hi += ph + (lo < pl);
+}
+
+// out[b][c][l][x] = base + sign * sum_{i<KIN, j<d} key[i][j][c][l][x] * dig[b][i][j][l][x]
+//   base = acc[b][c][l][x] (accumulate form) or, for the key switch,
+//   add_last[b][l][x] on the last component and 0 elsewhere; sign = -1 there.
+struct MacArgs {
+    uint64_t* out;
+    const uint64_t* acc;       // may alias out, or NULL
+    const uint64_t* add_last;  // [B][L][N] or NULL
+    const uint64_t* key;       // [KIN][d][KOUT][L][N]
+    const uint64_t* dig;       // [B][KIN][d][L][N]
+    const Barrett* bar;        // [L]
+    size_t B, N;
+    uint32_t KIN, KOUT, d, L, log_n;
+    int negate;
+};
+
+__global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
+    const size_t LN = (size_t)a.L * a.N;
+    const size_t total = a.B * a.KOUT * LN;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t lx = t % LN;                 // l * N + x
+        const uint32_t c = (uint32_t)((t / LN) % a.KOUT);
+        const size_t b = t / (LN * a.KOUT);
+        const uint32_t l = (uint32_t)(lx >> a.log_n);
+        const Barrett m = a.bar[l];
+        uint64_t lo = 0, hi = 0;
+        uint32_t terms = 0;
+        const uint64_t* kp = a.key + (size_t)c * LN + lx;
+        const uint64_t* dp = a.dig + b * a.KIN * a.d * LN + lx;
+        const size_t kstride = (size_t)a.KOUT * LN;
+        for (uint32_t ij = 0; ij < a.KIN * a.d; ++ij) {
+            mac128(lo, hi, __ldg(kp + ij * kstride), __ldg(dp + ij * LN));
+            if (++terms == 8) {  // products < 2^124: fold before the sum can reach 2^128
+                lo = barrett_reduce_2limb(lo, hi, m);
+                hi = 0;
+                terms = 1;
+            }
+        }
+        uint64_t s = barrett_reduce_2limb(lo, hi, m);
+        uint64_t r;
+        if (a.negate) {
+            uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
+            r = sub_mod(base, s, m.q);
+        } else {
+            uint64_t base = a.acc ? a.acc[t] : 0;
+            r = add_mod(base, s, m.q);
+        }
+        a.out[t] = r;
+    }
+}
+
+unsigned grid_for(size_t work, unsigned threads) {
+    const size_t cap = 148ull * 2048 / threads;
+    size_t b = (work + threads - 1) / threads;
+    return (unsigned)std::max<size_t>(1, std::min(b, cap));
+}
+
+int check_compat(const pg_ntt_table* t, const pg_gadget_basis* g) {
+    if (!t || !g) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL table or basis");
+    const pg_rns_base* b = gadget_base(g);
+    if (rns_L(b) != t->L) return set_error(PG_ERR_INVALID_ARGUMENT, "table and RNS base have different moduli counts");
+    const uint64_t* m = rns_moduli(b);
+    for (uint32_t l = 0; l < t->L; ++l)
+        if (m[l] != t->moduli[l]) return set_error(PG_ERR_INVALID_ARGUMENT, "table and RNS base moduli differ");
+    if (t->log_n > 16) return set_error(PG_ERR_UNSUPPORTED, "ring degree above 2^16");
+    return PG_OK;
+}
+
+// workspace: BigUint values [P][N][W] + lifted digits [P][d][L][N] (+ extra)
+size_t ws_bytes(const pg_ntt_table* t, const pg_gadget_basis* g, size_t polys, size_t extra_words) {
+    const pg_rns_base* b = gadget_base(g);
+    const size_t big = polys * t->n * rns_W(b);
+    const size_t dig = polys * gadget_d(g) * (size_t)t->L * t->n;
+    return (big + dig + extra_words) * sizeof(uint64_t) + 256;
+}
+
+struct Workspace {
+    void* ptr = nullptr;
+    bool owned = false;
+    cudaStream_t st = 0;
+    ~Workspace() {
+        if (owned && ptr) cudaFreeAsync(ptr, st);
+    }
+};
+
+int get_workspace(Workspace& w, void* given, size_t given_bytes, size_t need, cudaStream_t st) {
+    w.st = st;
+    if (given) {
+        if (given_bytes < need) return set_error(PG_ERR_INVALID_ARGUMENT, "workspace too small");
+        w.ptr = given;
+        return PG_OK;
+    }
+    cudaError_t e = cudaMallocAsync(&w.ptr, need, st);
+    if (e != cudaSuccess) return cuda_status(e, "workspace allocation");
+    w.owned = true;
+    return PG_OK;
+}
+
+// compose (when the input is CRT residues) + lifted digits + forward NTT of
+// every digit row; returns the digit buffer inside the workspace
+int digits_pipeline(const pg_ntt_table* t, const pg_gadget_basis* g, const uint64_t* in, bool in_is_crt,
+                    size_t polys, uint32_t ppg, size_t group_stride, uint64_t* ws, uint64_t** digits_out,
+                    cudaStream_t st) {
+    const pg_rns_base* b = gadget_base(g);
+    const size_t n = t->n;
+    const size_t count = polys * n;
+    uint64_t* big = ws;
+    uint64_t* dig = ws + count * rns_W(b);
+    const uint64_t* vals = in;
+    if (in_is_crt) {
+        int rc = launch_compose(b, in, big, count, n, ppg, group_stride, st);
+        if (rc) return rc;
+        vals = big;
+    }
+    int rc = launch_gadget(g, vals, dig, count, n, true, st);
+    if (rc) return rc;
+    rc = launch_ntt(make_args(t, dig, polys * gadget_d(g) * (size_t)t->L, 0), t->log_n, MODE_FWD, st);
+    if (rc) return rc;
+    *digits_out = dig;
+    return PG_OK;
+}
+
+int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t* acc, const uint64_t* add_last,
+               const uint64_t* key, const uint64_t* dig, size_t B, uint32_t kin, uint32_t kout, int negate,
+               cudaStream_t st) {
+    MacArgs a{};
+    a.out = out;
+    a.acc = acc;
+    a.add_last = add_last;
+    a.key = key;
+    a.dig = dig;
+    a.bar = t->d_barrett;
+    a.B = B;
+    a.N = t->n;
+    a.KIN = kin;
+    a.KOUT = kout;
+    a.d = d;
+    a.L = t->L;
+    a.log_n = t->log_n;
+    a.negate = negate;
+    const size_t total = B * kout * (size_t)t->L * t->n;
+    mac_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
+    count_launch();
+    PG_LAUNCH_CHECK("mac_kernel launch");
+    return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t pg_ext_product_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, size_t batch) {
+    if (!t || !g) return 0;
+    return ws_bytes(t, g, batch * (k + 1), 0);
+}
+
+int pg_ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
+                   const uint64_t* d_ggsw, uint64_t* d_out, size_t batch, void* d_ws, size_t ws_size, void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (batch == 0) return PG_OK;
+    if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t polys = batch * (k + 1);
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, 0), st);
+    if (rc) return rc;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_in, true, polys, k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)w.ptr, &dig, st);
+    if (rc) return rc;
+    return launch_mac(t, gadget_d(g), d_out, nullptr, nullptr, d_ggsw, dig, batch, k + 1, k + 1, 0, st);
+}
+
+int pg_glev_mac_crt_poly(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, uint64_t* d_acc,
+                         const uint64_t* d_glev, const uint64_t* d_crt_poly, void* d_ws, size_t ws_size,
+                         void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (!d_acc || !d_glev || !d_crt_poly) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, 1, 0), st);
+    if (rc) return rc;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_crt_poly, true, 1, 1, (size_t)t->L * t->n, (uint64_t*)w.ptr, &dig, st);
+    if (rc) return rc;
+    return launch_mac(t, gadget_d(g), d_acc, d_acc, nullptr, d_glev, dig, 1, 1, k + 1, 0, st);
+}
+
+int pg_glev_mac_big_uint_poly(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, uint64_t* d_acc,
+                              const uint64_t* d_glev, const uint64_t* d_big_poly, void* d_ws, size_t ws_size,
+                              void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (!d_acc || !d_glev || !d_big_poly) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, 1, 0), st);
+    if (rc) return rc;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_big_poly, false, 1, 1, 0, (uint64_t*)w.ptr, &dig, st);
+    if (rc) return rc;
+    return launch_mac(t, gadget_d(g), d_acc, d_acc, nullptr, d_glev, dig, 1, 1, k + 1, 0, st);
+}
+
+size_t pg_key_switch_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in, uint32_t k_out,
+                                    size_t batch) {
+    (void)k_out;
+    if (!t || !g) return 0;
+    return ws_bytes(t, g, batch * k_in, batch * (size_t)t->L * t->n);
+}
+
+int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in, uint32_t k_out,
+                  const uint64_t* d_key, const uint64_t* d_in, uint64_t* d_out, size_t batch, void* d_ws,
+                  size_t ws_size, void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (batch == 0) return PG_OK;
+    if (!d_key || !d_in || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (k_in == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k_in must be at least 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t LN = (size_t)t->L * t->n;
+    const size_t polys = batch * k_in;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, batch * LN), st);
+    if (rc) return rc;
+    uint64_t* ws = (uint64_t*)w.ptr;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_in, true, polys, k_in, (size_t)(k_in + 1) * LN, ws, &dig, st);
+    if (rc) return rc;
+    // b of every input, moved to the NTT domain (key_switch.rs:118-121)
+    uint64_t* bt = dig + polys * gadget_d(g) * LN;
+    PG_CUDA(cudaMemcpy2DAsync(bt, LN * 8, d_in + (size_t)k_in * LN, (size_t)(k_in + 1) * LN * 8, LN * 8, batch,
+                              cudaMemcpyDeviceToDevice, st));
+    rc = launch_ntt(make_args(t, bt, batch * t->L, 0), t->log_n, MODE_FWD, st);
+    if (rc) return rc;
+    // c_out = -(sum_i GLev_i (x) a_i) + (0, .., NTT(b))  (key_switch.rs:96-127)
+    return launch_mac(t, gadget_d(g), d_out, nullptr, bt, d_key, dig, batch, k_in, k_out + 1, 1, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+"""Python mirror of primus_rns / primus_decompose / primus_lattice operations
+over the C ABI (device buffers in, device buffers out).
+
+    RnsBase        RNSBase              primus_rns/src/base.rs
+    BaseConverter  BaseConverter        primus_rns/src/converter.rs
+    GadgetBasis    BigUintApproxSignedBasis  primus_decompose/src/big_integer/basis.rs
+    external_product  CrtGlwe::mul_dcrt_ggsw_inplace   primus_lattice/src/glwe/crt.rs:202
+    glev_mac_*        DcrtGlwe::add_dcrt_glev_mul_*     primus_lattice/src/glwe/dcrt.rs:170,249
+    key_switch        CrtGlweKeySwitchingKey::key_swithching_inplace  primus_fhe_core/src/key_switch.rs:79
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as nat
+from ._native import DeviceBuffer, PrimusGpuError, call, ptr
+
+
+def _sh(stream):
+    return None if stream is None else stream.h
+
+
+class RnsError(PrimusGpuError):
+    pass
+
+
+class RnsBase:
+    def __init__(self, moduli):
+        self.moduli = [int(q) for q in moduli]
+        m = np.asarray(self.moduli, dtype=np.uint64)
+        h = C.c_void_p()
+        st = nat.lib().pg_rns_base_create(ptr(m), len(self.moduli), C.byref(h))
+        if st != nat.PG_OK:
+            raise RnsError(st, "pg_rns_base_create", nat.lib().pg_last_error().decode())
+        self.h = h.value
+        L, W = C.c_uint32(), C.c_uint32()
+        call("pg_rns_base_info", self.h, C.byref(L), C.byref(W), None)
+        self.L, self.W = L.value, W.value
+        prod = np.zeros(self.W, np.uint64)
+        call("pg_rns_base_info", self.h, None, None, ptr(prod))
+        self.product = sum(int(v) << (64 * i) for i, v in enumerate(prod))
+
+    def moduli_count(self):
+        return self.L
+
+    def big_uint_value_len(self):
+        return self.W
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_rns_base_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compose(self, residues: DeviceBuffer, values: DeviceBuffer, count: int, stream=None):
+        call("pg_rns_compose", self.h, residues.ptr, values.ptr, count, _sh(stream))
+
+    def decompose(self, values: DeviceBuffer, residues: DeviceBuffer, count: int, stream=None):
+        call("pg_rns_decompose", self.h, values.ptr, residues.ptr, count, _sh(stream))
+
+    def wrapping_decompose_small(self, small: DeviceBuffer, residues: DeviceBuffer, count: int, small_modulus: int,
+                                 stream=None):
+        call("pg_rns_wrapping_decompose_small", self.h, small.ptr, residues.ptr, count, small_modulus, _sh(stream))
+
+
+class BaseConverter:
+    def __init__(self, ibase: RnsBase, obase: RnsBase):
+        self.ibase, self.obase = ibase, obase
+        h = C.c_void_p()
+        call("pg_base_converter_create", ibase.h, obase.h, C.byref(h))
+        self.h = h.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_base_converter_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fast_convert_array(self, x: DeviceBuffer, out: DeviceBuffer, n: int, stream=None):
+        call("pg_fast_convert_array", self.h, x.ptr, out.ptr, n, _sh(stream))
+
+
+class GadgetBasis:
+    def __init__(self, base: RnsBase, log_basis: int, reverse_length: int | None = None):
+        self.base = base
+        h = C.c_void_p()
+        call("pg_gadget_basis_create", base.h, log_basis, -1 if reverse_length is None else reverse_length,
+             C.byref(h))
+        self.h = h.value
+        d, drop = C.c_uint32(), C.c_uint32()
+        call("pg_gadget_basis_info", self.h, C.byref(d), C.byref(drop), None)
+        self.d, self.drop_bits, self.log_basis = d.value, drop.value, log_basis
+        self.scalar_residues = np.zeros((self.d, base.L), np.uint64)
+        call("pg_gadget_basis_info", self.h, None, None, ptr(self.scalar_residues))
+
+    def decompose_length(self):
+        return self.d
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_gadget_basis_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def decompose(self, values: DeviceBuffer, digits: DeviceBuffer, count: int, stream=None):
+        call("pg_gadget_decompose", self.h, values.ptr, digits.ptr, count, _sh(stream))
+
+    def decompose_lift(self, values: DeviceBuffer, residues: DeviceBuffer, count: int, stream=None):
+        call("pg_gadget_decompose_lift", self.h, values.ptr, residues.ptr, count, _sh(stream))
+
+
+def external_product(table, basis: GadgetBasis, k: int, glwe_in: DeviceBuffer, ggsw: DeviceBuffer,
+                     glwe_out: DeviceBuffer, batch: int, workspace: DeviceBuffer | None = None, stream=None):
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_ext_product", table.h, basis.h, k, glwe_in.ptr, ggsw.ptr, glwe_out.ptr, batch, ws, wsb, _sh(stream))
+
+
+def ext_product_workspace_size(table, basis: GadgetBasis, k: int, batch: int) -> int:
+    return int(nat.lib().pg_ext_product_workspace_size(table.h, basis.h, k, batch))
+
+
+def glev_mac_crt_poly(table, basis: GadgetBasis, k: int, acc: DeviceBuffer, glev: DeviceBuffer,
+                      crt_poly: DeviceBuffer, stream=None):
+    call("pg_glev_mac_crt_poly", table.h, basis.h, k, acc.ptr, glev.ptr, crt_poly.ptr, None, 0, _sh(stream))
+
+
+def glev_mac_big_uint_poly(table, basis: GadgetBasis, k: int, acc: DeviceBuffer, glev: DeviceBuffer,
+                           big_poly: DeviceBuffer, stream=None):
+    call("pg_glev_mac_big_uint_poly", table.h, basis.h, k, acc.ptr, glev.ptr, big_poly.ptr, None, 0, _sh(stream))
+
+
+def key_switch(table, basis: GadgetBasis, k_in: int, k_out: int, key: DeviceBuffer, c_in: DeviceBuffer,
+               c_out: DeviceBuffer, batch: int, workspace: DeviceBuffer | None = None, stream=None):
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_key_switch", table.h, basis.h, k_in, k_out, key.ptr, c_in.ptr, c_out.ptr, batch, ws, wsb, _sh(stream))
