@@ -283,6 +283,20 @@ int pg_key_switch(const pg_ntt_table *table, const pg_gadget_basis *basis, uint3
                   uint32_t k_out, const uint64_t *d_key, const uint64_t *d_c_in,
                   uint64_t *d_c_out, size_t batch, void *d_workspace, size_t workspace_bytes,
                   void *stream);
+/* pg_ext_product for callers that cannot allocate device memory when they
+ * call (hosts holding only device pointers owned by another runtime, serving
+ * processes that reserve HBM at start-up and forbid later allocations).  No
+ * counterpart in the reference: it exists for this library's C callers.  The
+ * scratch is a fixed 32 MiB device array inside the library, held by every GPU
+ * that loads it until the process exits; batches needing more are rejected
+ * with PG_ERR_UNSUPPORTED and a message giving the largest batch of that shape.
+ * The first call on each device looks up the array's device address, so make
+ * that first call before any stream capture.  No scratch word needs to start
+ * at zero, but every call shares the array: calls whose work overlaps on the
+ * GPU (other streams, other threads) race, so serialise them. */
+int pg_ext_product_noalloc(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                           const uint64_t *d_glwe_in, const uint64_t *d_ggsw,
+                           uint64_t *d_glwe_out, size_t batch, void *stream);
 
 /* ------------------------------------------------------- seeded inputs
  * Device-side fill with the counter-based generator (uniform below q_l per

@@ -18,6 +18,8 @@
 // accumulator.  Outputs are canonical NTT-domain residues, equal to the
 // reference's sequential per-digit MAC.
 #include <algorithm>
+#include <cstdio>
+#include <mutex>
 
 #include "internal.hpp"
 
@@ -189,6 +191,43 @@ int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t*
     return PG_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// External product without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they call: hosts
+// that only receive device pointers from another runtime and hold no CUDA
+// allocator of their own (FFI wrappers around buffers someone else owns), and
+// serving processes that reserve their HBM budget at start-up and forbid
+// allocations afterwards, because cudaMalloc / cudaFree synchronize the device
+// and can fail under memory pressure in the middle of a request.  For them the
+// scratch of the external product lives in the file-scope array below: a fixed
+// 32 MiB that every GPU which loads this library holds until the process exits.
+// Host code cannot use the array's name as a device address (it is a host-side
+// stand-in), so the device address is fetched once per device with
+// cudaGetSymbolAddress, with that device current.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = 32ull << 20;
+static __device__ __align__(256) uint64_t g_noalloc_scratch[kNoAllocScratchBytes / sizeof(uint64_t)];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[128] = {};
+
+// device address of g_noalloc_scratch on the current device (set up on first use)
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    PG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) return set_error(PG_ERR_UNSUPPORTED, "device ordinal above 127");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return PG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -280,6 +319,35 @@ int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in
     if (rc) return rc;
     // c_out = -(sum_i GLev_i (x) a_i) + (0, .., NTT(b))  (key_switch.rs:96-127)
     return launch_mac(t, gadget_d(g), d_out, nullptr, bt, d_key, dig, batch, k_in, k_out + 1, 1, st);
+}
+
+// Same computation and outputs as pg_ext_product, with its scratch in the
+// library's fixed device array instead of caller or runtime allocations.
+int pg_ext_product_noalloc(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
+                           const uint64_t* d_ggsw, uint64_t* d_out, size_t batch, void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (batch == 0) return PG_OK;
+    if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    const size_t need = ws_bytes(t, g, batch * (k + 1), 0);
+    if (need > kNoAllocScratchBytes) {
+        const size_t per = ws_bytes(t, g, (size_t)(k + 1), 0);
+        char buf[256];
+        snprintf(buf, sizeof buf,
+                 "pg_ext_product_noalloc: this batch needs %zu bytes of scratch, above the fixed %zu bytes; "
+                 "submit at most %zu ciphertexts of this shape per call",
+                 need, kNoAllocScratchBytes, per ? kNoAllocScratchBytes / per : (size_t)0);
+        return set_error(PG_ERR_UNSUPPORTED, buf);
+    }
+    void* ws = nullptr;
+    rc = noalloc_scratch(&ws);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_in, true, batch * (k + 1), k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)ws,
+                         &dig, st);
+    if (rc) return rc;
+    return launch_mac(t, gadget_d(g), d_out, nullptr, nullptr, d_ggsw, dig, batch, k + 1, k + 1, 0, st);
 }
 
 }  // extern "C"
