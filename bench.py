@@ -321,7 +321,7 @@ def run_gpu(args):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,
-                         "kernel": "ntt_cluster_kernel<16,13,4,RT> (fused fwd -> x plain -> inv)",
+                         "kernel": "ntt_cluster_kernel<16,12,4,RT,fast> (fused fwd -> x plain -> inv)",
                          "algorithmic_bytes_per_launch": ALGO_BYTES},
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
