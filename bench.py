@@ -310,6 +310,11 @@ def run_gpu(args):
             v, sample, thr = cpu_reference(O.ntt_primes(1 << 50, 2 * N, L), seconds_target=args.cpu_seconds)
             cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
                    "sample": "C restatement of UintNttTable/DcrtPolynomial (oracle), OpenMP over rows; " + sample}
+        workloads = None
+        if world == 1 and not args.no_extra:
+            workloads = {"polymul_n1024": bench_polymul_1024(P, stream),
+                         "uneven_batch": bench_uneven(P, stream),
+                         "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu)}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
@@ -326,11 +331,117 @@ def run_gpu(args):
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
             "cpu_baseline": cpu,
+            "workloads": workloads,
         }
         print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+# --------------------------------------------------------------------------
+# Secondary workloads of the same path, reported beside the headline number.
+# --------------------------------------------------------------------------
+def _time_stream(P, stream, fn, reps):
+    e0, e1 = P.Event(), P.Event()
+    fn()
+    stream.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    stream.synchronize()
+    return e0.elapsed_ms(e1) / reps
+
+
+def bench_polymul_1024(P, stream):
+    """64 pairs of N = 1024 polys, q = largest prime < 2^50 with q = 1 mod 2048:
+    forward both, pointwise product, inverse (one graph-replayed submission)."""
+    q = P.prev_prime_congruent(1 << 50, 2048)
+    tab = P.DcrtTable(10, [q])
+    batch = P.PolymulBatch([tab])
+    a = P.DeviceBuffer(64 * 1024)
+    b = P.DeviceBuffer(64 * 1024)
+    tab.fill_uniform(a, 64, seed=0x5EED0000, stream=stream)
+    tab.fill_uniform(b, 64, seed=0x5EED0100, stream=stream)
+    jobs = [(_Slice(a, i * 1024), _Slice(b, i * 1024), 10, 1) for i in range(64)]
+    ms = _time_stream(P, stream, lambda: batch.run(jobs, use_graph=True, stream=stream), 50)
+    one = [jobs[0]]
+    ms_one = _time_stream(P, stream, lambda: batch.run(one, use_graph=False, stream=stream), 50)
+    return {"workload": "64 products of N=1024 polys (q < 2^50, q = 1 mod 2048): fwd x2, mul, inv",
+            "batch_latency_us": ms * 1e3, "pairs_per_s": 64 / (ms / 1e3),
+            "single_pair_latency_us": ms_one * 1e3}
+
+
+class _Slice:
+    """a view into a DeviceBuffer at an element offset (for job descriptors)"""
+
+    def __init__(self, buf, off):
+        self.buf, self.ptr = buf, buf.ptr + 8 * off
+
+
+def bench_uneven(P, stream, jobs_n=512):
+    """512 products with N uniform in {2^10..2^16} and L uniform in 1..32
+    (primes < 2^50, q = 1 mod 2N, descending), one graph-replayed submission
+    vs one call per job."""
+    rng = np.random.default_rng(0x5EED0002)
+    log_ns = list(range(10, 17))
+    shape = [(int(rng.choice(log_ns)), int(rng.integers(1, 33))) for _ in range(jobs_n)]
+    tables = {ln: P.DcrtTable(ln, P.ntt_primes(1 << 50, 2 << ln, 32)) for ln in log_ns}
+    batch = P.PolymulBatch(list(tables.values()))
+    jobs, total_bytes = [], 0
+    for j, (ln, L) in enumerate(shape):
+        n = 1 << ln
+        t = tables[ln]
+        # buffers hold all 32 limbs so the device generator fills them in one call;
+        # the job uses the first L
+        a, b = P.DeviceBuffer(t.L * n), P.DeviceBuffer(t.L * n)
+        t.fill_uniform(a, 1, seed=0x5EED0003, stream0=64 * j, stream=stream)
+        t.fill_uniform(b, 1, seed=0x5EED0004, stream0=64 * j, stream=stream)
+        jobs.append((a, b, ln, L))
+        total_bytes += 24 * n * L
+    stream.synchronize()
+    ms_graph = _time_stream(P, stream, lambda: batch.run(jobs, use_graph=True, stream=stream), 10)
+    ms_plain = _time_stream(P, stream, lambda: [batch.run([j], use_graph=False, stream=stream) for j in jobs], 3)
+    return {"workload": "512 products, N uniform in 2^10..2^16, L uniform in 1..32, one graph launch",
+            "jobs": jobs_n, "ms_per_batch": ms_graph, "jobs_per_s": jobs_n / (ms_graph / 1e3),
+            "algorithmic_gb": total_bytes / 1e9, "achieved_gbs": total_bytes / (ms_graph / 1e3) / 1e9,
+            "plain_per_job_ms": ms_plain, "plain_jobs_per_s": jobs_n / (ms_plain / 1e3)}
+
+
+def bench_ext_product(P, stream, batch=4096, cpu=False):
+    """GLWE x GGSW external products: N = 2048, q = largest prime < 2^54 with
+    q = 1 mod 4096, log_basis 7 (7 digits), k = 1, L = 1, one GGSW, 4096 ciphertexts."""
+    q = P.prev_prime_congruent(1 << 54, 4096)
+    tab = P.DcrtTable(11, [q])
+    g = P.GadgetBasis(P.RnsBase([q]), 7)
+    k, n = 1, 2048
+    ggsw = P.DeviceBuffer((k + 1) * g.d * (k + 1) * n)
+    glwe = P.DeviceBuffer(batch * (k + 1) * n)
+    out = P.DeviceBuffer(batch * (k + 1) * n)
+    tab.fill_uniform(ggsw, (k + 1) * g.d * (k + 1), seed=0x5EED0004, stream=stream)
+    tab.fill_uniform(glwe, batch * (k + 1), seed=0x5EED0005, stream=stream)
+    ws = P.DeviceBuffer(P.ext_product_workspace_size(tab, g, k, batch) // 8 + 1)
+    ms = _time_stream(P, stream, lambda: P.external_product(tab, g, k, glwe, ggsw, out, batch, workspace=ws,
+                                                            stream=stream), 10)
+    res = {"workload": "GLWE x GGSW external product, N=2048, q < 2^54, B = 2^7, d = 7, k = 1, 4096 ciphertexts",
+           "ms_per_batch": ms, "ext_products_per_s": batch / (ms / 1e3)}
+    if cpu:
+        import oracle as O
+        t0 = time.perf_counter()
+        ot = O.DcrtTable(11, [q])
+        ob = O.RnsBase([q])
+        og = O.GadgetBasis(ob, 7)
+        lat = O.Lattice(ot, ob, og)
+        sample = 256
+        gg = O.uniform(1, 1, q, (k + 1) * og.d * (k + 1) * n)
+        ct = O.uniform(2, 2, q, sample * (k + 1) * n)
+        t0 = time.perf_counter()
+        lat.external_product(k, ct, gg, batch=sample, threads=cpu_threads())
+        dt = time.perf_counter() - t0
+        res["cpu_port_ext_products_per_s"] = sample / dt
+        res["cpu_port_sample"] = f"{sample} ciphertexts on {cpu_threads()} threads, {dt:.2f} s"
+    return res
 
 
 def main(argv=None):
@@ -340,6 +451,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="primus_b200", choices=["primus_b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--polys", type=int, default=POLYS,
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")

@@ -298,6 +298,31 @@ int pg_ext_product_noalloc(const pg_ntt_table *table, const pg_gadget_basis *bas
                            const uint64_t *d_glwe_in, const uint64_t *d_ggsw,
                            uint64_t *d_glwe_out, size_t batch, void *stream);
 
+/* ----------------------------------------------- uneven batches of products
+ * A job multiplies two coefficient-form DCRT polys of its own ring degree:
+ * a <- a * b (negacyclic), b <- NTT(b), using the first moduli_count primes of
+ * the batch's table for that degree -- per limb the reference's
+ * transform_slice x2, mul_assign, inverse_transform_slice
+ * (primus_ntt/src/ntt/primitive.rs:234-296, primus_poly/src/dcrt/mul.rs:97-110).
+ * One run launches, per ring degree present, a forward NTT over every a- and
+ * b-row and a fused multiply + inverse NTT over every a-row, the degrees on
+ * parallel streams.  With use_graph the first run of a job shape is captured
+ * into a CUDA graph and later runs of the same shape replay it. */
+typedef struct pg_polymul_job {
+    uint64_t *d_a;          /* [moduli_count][N], result */
+    uint64_t *d_b;          /* [moduli_count][N], left in the NTT domain */
+    uint32_t log_n;
+    uint32_t moduli_count;
+} pg_polymul_job;
+typedef struct pg_polymul_batch pg_polymul_batch;
+
+/* tables: one per ring degree (distinct log_n), each with enough primes */
+int pg_polymul_batch_create(const pg_ntt_table *const *tables, uint32_t table_count,
+                            pg_polymul_batch **out);
+int pg_polymul_batch_destroy(pg_polymul_batch *batch);
+int pg_polymul_batch_run(pg_polymul_batch *batch, const pg_polymul_job *h_jobs, size_t count,
+                         int use_graph, void *stream);
+
 /* ------------------------------------------------------- seeded inputs
  * Device-side fill with the counter-based generator (uniform below q_l per
  * limb; stream id = stream0 + poly*L + limb). */

@@ -75,6 +75,16 @@ struct pg_ntt_table {
 };
 
 namespace pg {
+// one row of a descriptor-driven (ragged) NTT launch: the row's data, its limb
+// in the table and, for inverse launches, an optional NTT-domain multiplicand
+// applied before the transform
+struct RowDesc {
+    uint64_t* data;
+    const uint64_t* mul;
+    uint32_t limb;
+    uint32_t pad;
+};
+
 // kernel argument block for the NTT family
 struct NttArgs {
     uint64_t* data;
@@ -86,6 +96,7 @@ struct NttArgs {
     const uint64_t* plain;
     const uint64_t* plain_q;
     const Barrett* bar;
+    const RowDesc* desc;  // NULL: rows are [polys][L][N] at data
     uint64_t rows;
     uint64_t max_modulus;
     uint32_t L;
@@ -105,6 +116,7 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     a.plain = nullptr;
     a.plain_q = nullptr;
     a.bar = t->d_barrett;
+    a.desc = nullptr;
     a.rows = rows;
     a.max_modulus = 0;
     for (uint64_t m : t->moduli) a.max_modulus = m > a.max_modulus ? m : a.max_modulus;

@@ -289,11 +289,18 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     // concurrently running CTAs share one prime's twiddles in L2
     const uint64_t u = (uint64_t)blockIdx.x * ROWS + threadIdx.y;
     const bool active = u < a.rows;
-    const uint64_t polys = a.rows / a.L;
-    const uint32_t limb = active ? (uint32_t)(u / polys) : 0;
+    const uint64_t polys = a.desc ? 1 : a.rows / a.L;  // descriptor rows need no [P][L] shape
+    uint32_t limb = active ? (uint32_t)(u / polys) : 0;
     const uint64_t row = active ? (u % polys) * a.L + limb : 0;
     uint64_t* sm = smem_block + threadIdx.y * padded(N);
     uint64_t* g = a.data + row * N;
+    const uint64_t* mulp = nullptr;
+    if (a.desc) {  // descriptor-driven rows (ragged batches)
+        const RowDesc d = a.desc[active ? u : 0];
+        g = d.data;
+        limb = d.limb;
+        mulp = d.mul;
+    }
     const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
     uint64_t x[E];
 
@@ -340,7 +347,12 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
         if constexpr (MODE == MODE_INV) {
             // stage the bit-reversed row through smem (coalesced), then round 0
 #pragma unroll
-            for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = active ? g[tid + k * T] : 0;
+            for (int k = 0; k < E; ++k) {
+                uint64_t v = active ? g[tid + k * T] : 0;
+                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+                if (mulp && active) v = barrett_mul(v, mulp[tid + k * T], a.bar[limb]);
+                sm[padi(tid + k * T)] = v;
+            }
             __syncthreads();
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         } else {
@@ -407,10 +419,17 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
     // grid is exactly rows * C; clusters run limb-major so that concurrently
     // running clusters share one prime's twiddles in L2
     const uint64_t u = blockIdx.x >> LOG_C;
-    const uint64_t polys = a.rows / a.L;
-    const uint32_t limb = (uint32_t)(u / polys);
+    const uint64_t polys = a.desc ? 1 : a.rows / a.L;  // descriptor rows need no [P][L] shape
+    uint32_t limb = (uint32_t)(u / polys);
     const uint64_t row = (u % polys) * a.L + limb;
     uint64_t* g = a.data + row * N;
+    const uint64_t* mulp = nullptr;
+    if (a.desc) {  // descriptor-driven rows (ragged batches)
+        const RowDesc d = a.desc[u];
+        g = d.data;
+        limb = d.limb;
+        mulp = d.mul;
+    }
     const uint64_t q = a.moduli[limb], nq = 0 - q;
     const uint32_t gt = (rank << LOG_T) + tid;  // cross group (column) of this thread
     uint64_t x[E];
@@ -469,7 +488,12 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         if constexpr (MODE == MODE_INV) {
             uint64_t* gb = g + rank * M;
 #pragma unroll
-            for (int k = 0; k < E; ++k) sm[padi(tid + k * T)] = gb[tid + k * T];
+            for (int k = 0; k < E; ++k) {
+                uint64_t v = gb[tid + k * T];
+                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+                if (mulp) v = barrett_mul(v, mulp[rank * M + tid + k * T], a.bar[limb]);
+                sm[padi(tid + k * T)] = v;
+            }
             __syncthreads();
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         }

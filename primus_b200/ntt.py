@@ -214,3 +214,35 @@ class NttTable(DcrtTable):
     @classmethod
     def new(cls, log_n: int, modulus: int):
         return cls(log_n, modulus)
+
+
+class PolymulJob(C.Structure):
+    _fields_ = [("d_a", C.c_void_p), ("d_b", C.c_void_p), ("log_n", C.c_uint32), ("moduli_count", C.c_uint32)]
+
+
+class PolymulBatch:
+    """Uneven batches of products a <- a*b over several ring degrees in one
+    (graph-captured) submission; one table per degree (pg_polymul_batch_*)."""
+
+    def __init__(self, tables):
+        self.tables = list(tables)
+        arr = (C.c_void_p * len(self.tables))(*[t.h for t in self.tables])
+        h = C.c_void_p()
+        call("pg_polymul_batch_create", arr, len(self.tables), C.byref(h))
+        self.h = h.value
+
+    def run(self, jobs, use_graph=True, stream=None):
+        """jobs: iterable of (a: DeviceBuffer, b: DeviceBuffer, log_n, moduli_count)."""
+        arr = (PolymulJob * len(jobs))(*[PolymulJob(a.ptr, b.ptr, ln, L) for a, b, ln, L in jobs])
+        call("pg_polymul_batch_run", self.h, arr, len(jobs), int(bool(use_graph)), _sh(stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_polymul_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
