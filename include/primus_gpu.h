@@ -323,6 +323,68 @@ int pg_polymul_batch_destroy(pg_polymul_batch *batch);
 int pg_polymul_batch_run(pg_polymul_batch *batch, const pg_polymul_job *h_jobs, size_t count,
                          int use_graph, void *stream);
 
+/* ------------------------------------------------------- request server
+ * Continuous batching of mixed requests on one GPU (no reference counterpart:
+ * the reference is a library of synchronous calls).  Clients keep keys and
+ * ciphertexts resident in device memory and submit single requests; a worker
+ * thread forms batches of one kind and shape whenever one of its slots (a
+ * stream plus an equal share of memory_budget_bytes of scratch) is free, taking
+ * as many pending requests as fit the slot's scratch (admission by memory), so
+ * requests that arrive while others run join the next batch and batches on
+ * different slots overlap.  Completion is signalled by a host callback on the
+ * slot's stream.  Results are identical to running each request alone. */
+enum { PG_REQ_POLYMUL = 1, PG_REQ_EXT_PRODUCT = 2, PG_REQ_KEY_SWITCH = 3 };
+
+typedef struct pg_request {
+    int kind;
+    uint32_t key;            /* ext product / key switch: id from pg_server_register_key */
+    uint64_t *d_a;           /* polymul: a <- a * b, b <- NTT(b) (pg_polymul_job) */
+    uint64_t *d_b;
+    uint32_t log_n;
+    uint32_t moduli_count;
+    const uint64_t *d_in;    /* ext product / key switch: one ciphertext in ... */
+    uint64_t *d_out;         /* ... and its result (NTT domain) */
+} pg_request;
+
+typedef struct pg_server_config {
+    size_t memory_budget_bytes; /* scratch shared by the slots */
+    uint32_t slots;             /* concurrent batches (streams), 1..64 */
+    uint32_t max_batch;         /* requests per batch */
+    uint32_t max_queue;         /* pending requests before submit rejects (0: 2^20) */
+} pg_server_config;
+
+typedef struct pg_server_stats {
+    uint64_t submitted, completed, rejected, batches;
+    double mean_batch, p50_us, p99_us, max_us; /* latency = submit -> completion */
+} pg_server_stats_t;
+
+typedef struct pg_server pg_server;
+
+/* polymul_tables: one per ring degree polymul requests may use */
+int pg_server_create(const pg_server_config *config, const pg_ntt_table *const *polymul_tables,
+                     uint32_t table_count, pg_server **out);
+/* stops the worker; drain first so that no request is left pending */
+int pg_server_destroy(pg_server *server);
+/* a GGSW (kind PG_REQ_EXT_PRODUCT, k_out ignored) or key-switching key
+ * (PG_REQ_KEY_SWITCH) resident on the device; the layouts of pg_ext_product /
+ * pg_key_switch */
+int pg_server_register_key(pg_server *server, int kind, const pg_ntt_table *table,
+                           const pg_gadget_basis *basis, uint32_t k_in, uint32_t k_out,
+                           const uint64_t *d_key, uint32_t *key_id);
+/* queue one request; PG_ERR_REJECTED when the queue is full or the request
+ * cannot fit one slot's scratch, PG_ERR_INVALID_ARGUMENT when malformed */
+int pg_server_submit(pg_server *server, const pg_request *request, uint64_t *ticket);
+/* wait for a request (timeout_us < 0: no limit); PG_ERR_TIMEOUT if not done */
+int pg_server_wait(pg_server *server, uint64_t ticket, int64_t timeout_us, double *latency_us);
+/* wait until nothing is pending or running */
+int pg_server_drain(pg_server *server, int64_t timeout_us);
+int pg_server_stats(pg_server *server, pg_server_stats_t *out, int reset);
+/* load replay: submit requests[i] at arrival_us[i] microseconds after the call
+ * (from the calling thread), wait for all; latency_us[i] = completion time minus
+ * scheduled arrival (-1 when rejected) */
+int pg_server_replay(pg_server *server, const pg_request *requests, const double *arrival_us,
+                     size_t count, double *latency_us);
+
 /* ------------------------------------------------------- seeded inputs
  * Device-side fill with the counter-based generator (uniform below q_l per
  * limb; stream id = stream0 + poly*L + limb). */

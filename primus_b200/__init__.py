@@ -8,6 +8,8 @@ from ._native import (DeviceBuffer, Event, PrimusGpuError, Stream, device_count,
                       synchronize)
 from .lattice import (BaseConverter, GadgetBasis, RnsBase, RnsError, external_product,  # noqa: F401
                       ext_product_workspace_size, glev_mac_big_uint_poly, glev_mac_crt_poly, key_switch)
+from .server import (Request, Server, ext_product_request, key_switch_request,  # noqa: F401
+                     polymul_request)
 from .ntt import (DcrtTable, NttError, NttTable, PolymulBatch, host_tables, minimal_primitive_root,  # noqa: F401
                   ntt_primes, prev_prime_congruent)
 
@@ -15,5 +17,6 @@ __all__ = [
     "DcrtTable", "NttTable", "NttError", "DeviceBuffer", "Stream", "Event", "PrimusGpuError",
     "ntt_primes", "prev_prime_congruent", "minimal_primitive_root", "host_tables", "device_count",
     "launch_count", "synchronize", "RnsBase", "RnsError", "BaseConverter", "GadgetBasis", "external_product",
-    "ext_product_workspace_size", "glev_mac_crt_poly", "glev_mac_big_uint_poly", "key_switch", "PolymulBatch",
+    "ext_product_workspace_size", "glev_mac_crt_poly", "glev_mac_big_uint_poly", "key_switch", "PolymulBatch", "Server", "Request",
+    "polymul_request", "ext_product_request", "key_switch_request",
 ]
