@@ -314,7 +314,8 @@ def run_gpu(args):
         if world == 1 and not args.no_extra:
             workloads = {"polymul_n1024": bench_polymul_1024(P, stream),
                          "uneven_batch": bench_uneven(P, stream),
-                         "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu)}
+                         "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu),
+                         "served_mixed": bench_served(P, stream)}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
@@ -443,6 +444,129 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
         res["cpu_port_sample"] = f"{sample} ciphertexts on {cpu_threads()} threads, {dt:.2f} s"
     return res
 
+
+def bench_served(P, stream, count=2000, seed=0x5EED0005):
+    """Mixed request stream: 50% RNS polymul (N = 2^12..2^16, L = 4..24), 30%
+    external product (the N = 2048 shape above), 20% key switch (N = 2^15, L = 16,
+    BigUint gadget with log_basis 49 -> 16 digits, k = 1).  The plain form runs
+    each request as its own synchronous call; the served form replays the same
+    trace into the continuous-batching server at Poisson arrival rates."""
+    rng = np.random.default_rng(seed)
+    pm_lns = list(range(12, 17))
+    pm_tables = {ln: P.DcrtTable(ln, P.ntt_primes(1 << 50, 2 << ln, 24)) for ln in pm_lns}
+    pm_batch = P.PolymulBatch(list(pm_tables.values()))
+    xq = P.prev_prime_congruent(1 << 54, 4096)
+    xt = P.DcrtTable(11, [xq])
+    xg = P.GadgetBasis(P.RnsBase([xq]), 7)
+    xkey = P.DeviceBuffer(2 * xg.d * 2 * 2048)
+    xt.fill_uniform(xkey, 2 * xg.d * 2, seed=seed + 1, stream=stream)
+    ks_moduli = P.ntt_primes(1 << 50, 1 << 16, 16)
+    kt = P.DcrtTable(15, ks_moduli)
+    kg = P.GadgetBasis(P.RnsBase(ks_moduli), 49)
+    kkey = P.DeviceBuffer(kg.d * 2 * 16 * 32768)
+    kt.fill_uniform(kkey, kg.d * 2, seed=seed + 2, stream=stream)
+    kinds = rng.choice(3, size=count, p=[0.5, 0.3, 0.2])
+    trace = []  # (kind, buffers...)
+    for i, kd in enumerate(kinds):
+        if kd == 0:
+            ln, L = int(rng.choice(pm_lns)), int(rng.integers(4, 25))
+            t = pm_tables[ln]
+            a, b = P.DeviceBuffer(t.L << ln), P.DeviceBuffer(t.L << ln)
+            t.fill_uniform(a, 1, seed=seed + 3, stream0=64 * i, stream=stream)
+            t.fill_uniform(b, 1, seed=seed + 4, stream0=64 * i, stream=stream)
+            trace.append(("pm", a, b, ln, L))
+        elif kd == 1:
+            di, do = P.DeviceBuffer(2 * 2048), P.DeviceBuffer(2 * 2048)
+            xt.fill_uniform(di, 2, seed=seed + 5, stream0=2 * i, stream=stream)
+            trace.append(("xp", di, do))
+        else:
+            di, do = P.DeviceBuffer(2 * 16 * 32768), P.DeviceBuffer(2 * 16 * 32768)
+            kt.fill_uniform(di, 2, seed=seed + 6, stream0=32 * i, stream=stream)
+            trace.append(("ks", di, do))
+    stream.synchronize()
+
+    # ---- plain: one synchronous call per request, in arrival order
+    def plain_call(it):
+        if it[0] == "pm":
+            pm_batch.run([(it[1], it[2], it[3], it[4])], use_graph=False, stream=stream)
+        elif it[0] == "xp":
+            P.external_product(xt, xg, 1, it[1], xkey, it[2], 1, stream=stream)
+        else:
+            P.key_switch(kt, kg, 1, 1, kkey, it[1], it[2], 1, stream=stream)
+
+    for it in trace[:50]:
+        plain_call(it)
+    stream.synchronize()
+    e0, e1 = P.Event(), P.Event()
+    service = np.zeros(count)
+    t_all = time.perf_counter()
+    for i, it in enumerate(trace):
+        e0.record(stream)
+        plain_call(it)
+        e1.record(stream)
+        stream.synchronize()
+        service[i] = e0.elapsed_ms(e1) * 1e3
+    plain_wall = time.perf_counter() - t_all
+    plain_rps = count / plain_wall
+    kind_names = {"pm": "polymul", "xp": "ext_product", "ks": "key_switch"}
+    per_kind = {}
+    for key, name in kind_names.items():
+        sel = np.array([it[0] == key for it in trace])
+        per_kind[name] = {"count": int(sel.sum()), "gpu_service_p50_us": float(np.percentile(service[sel], 50))}
+
+    def plain_replay(arrivals):
+        # a single FIFO worker running each request as its own synchronous call
+        lat = np.zeros(count)
+        t0 = time.perf_counter()
+        for i, it in enumerate(trace):
+            target = t0 + arrivals[i] * 1e-6
+            while time.perf_counter() < target:
+                pass
+            plain_call(it)
+            stream.synchronize()
+            lat[i] = (time.perf_counter() - target) * 1e6
+        return lat, time.perf_counter() - t0
+
+    # ---- served
+    srv = P.Server(memory_budget_bytes=8 << 30, slots=4, max_batch=512, polymul_tables=list(pm_tables.values()))
+    xid = srv.register_key(2, xt, xg, 1, 1, xkey)
+    kid = srv.register_key(3, kt, kg, 1, 1, kkey)
+    reqs = []
+    for it in trace:
+        if it[0] == "pm":
+            reqs.append(P.polymul_request(it[1], it[2], it[3], it[4]))
+        elif it[0] == "xp":
+            reqs.append(P.ext_product_request(xid, it[1], it[2]))
+        else:
+            reqs.append(P.key_switch_request(kid, it[1], it[2]))
+    # warm-up: the whole trace at once, then at twice the plain rate
+    srv.replay(reqs, np.zeros(count))
+    srv.replay(reqs, np.cumsum(rng.exponential(1e6 / (2 * plain_rps), count)))
+    srv.stats(reset=True)
+
+    def summary(lat, wall, offered):
+        ok = lat[lat >= 0]
+        return {"offered_rps": offered, "throughput_rps": len(ok) / wall, "p50_us": float(np.percentile(ok, 50)),
+                "p99_us": float(np.percentile(ok, 99)), "rejected": int((lat < 0).sum())}
+
+    plain_runs, served_runs = [], []
+    for mult in (0.5, 0.9, 2.0, 4.0, 8.0, None):
+        offered = None if mult is None else plain_rps * mult
+        arrivals = np.zeros(count) if mult is None else np.cumsum(rng.exponential(1e6 / offered, count))
+        if mult is not None and mult < 1:
+            lat, wall = plain_replay(arrivals)
+            plain_runs.append(summary(lat, wall, offered))
+        t0 = time.perf_counter()
+        lat = srv.replay(reqs, arrivals)
+        served_runs.append(summary(lat, time.perf_counter() - t0, offered))
+        served_runs[-1]["mean_batch"] = srv.stats(reset=True)["mean_batch"]
+    srv.close()
+    best = max(r["throughput_rps"] for r in served_runs)
+    return {"workload": "served mixed stream: 50% polymul N=2^12..2^16 L=4..24, 30% ext product (N=2048, k=1, "
+                        "7-bit gadget), 20% key switch (N=2^15, L=16, 49-bit gadget, 16 digits); Poisson arrivals",
+            "requests": count, "plain_capacity_rps": plain_rps, "per_kind": per_kind,
+            "plain": plain_runs, "served": served_runs, "served_max_rps": best,
+            "served_over_plain_capacity": best / plain_rps}
 
 def main(argv=None):
     ap = argparse.ArgumentParser()

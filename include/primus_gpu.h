@@ -76,6 +76,11 @@ int pg_event_record(void *event, void *stream);
 int pg_event_elapsed_ms(void *start, void *stop, float *ms);
 /* number of kernels this library has launched in this process */
 uint64_t pg_launch_count(void);
+/* Scratch that entry points allocate for themselves (when the caller passes no
+ * workspace) comes from a per-device pool that keeps freed memory for reuse.
+ * Trim the current device's pool to at most keep_bytes of unused memory.
+ * No reference counterpart: the reference allocates scratch on the heap. */
+int pg_scratch_trim(size_t keep_bytes);
 
 /* --------------------------------------------------------- number theory
  * Host helpers used to pick NTT-friendly primes the way the workloads do. */

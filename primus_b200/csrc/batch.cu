@@ -33,7 +33,8 @@ struct pg_polymul_batch {
     cudaStream_t streams[kClasses] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t joins[kClasses] = {};
-    cudaEvent_t copied = nullptr;  // host descriptors may be rewritten once this completes
+    cudaEvent_t copied = nullptr;    // host descriptors may be rewritten once this completes
+    cudaEvent_t finished = nullptr;  // the last call's launches (and so its descriptor reads) are done
     RowDesc* h_desc = nullptr;     // pinned
     RowDesc* d_desc = nullptr;
     size_t cap = 0;
@@ -115,6 +116,7 @@ int pg_polymul_batch_create(const pg_ntt_table* const* tables, uint32_t table_co
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->finished, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         pg_polymul_batch_destroy(b);
         return cuda_status(e, "pg_polymul_batch_create");
@@ -132,8 +134,9 @@ int pg_polymul_batch_destroy(pg_polymul_batch* b) {
     }
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->copied) cudaEventDestroy(b->copied);
+    if (b->finished) cudaEventDestroy(b->finished);
     cudaFreeHost(b->h_desc);
-    cudaFree(b->d_desc);
+    cudaFree(b->d_desc);  // also frees stream-ordered allocations (synchronizing)
     delete b;
     return PG_OK;
 }
@@ -168,15 +171,20 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
     // the previous call's descriptor copy must have left the pinned buffer
     PG_CUDA(cudaEventSynchronize(b->copied));
     if (total > b->cap) {
+        // grow geometrically; the device copy is stream-ordered so that growing
+        // does not wait for work other streams have in flight
         destroy_graph(b);  // captured launches point at the old descriptor buffer
+        const size_t cap = std::max<size_t>(std::max<size_t>(total, 2 * b->cap), 4096);
         cudaFreeHost(b->h_desc);
-        cudaFree(b->d_desc);
+        if (b->d_desc) {
+            PG_CUDA(cudaStreamWaitEvent(st, b->finished, 0));  // the last call may have used another stream
+            PG_CUDA(cudaFreeAsync(b->d_desc, st));
+        }
         b->h_desc = nullptr;
         b->d_desc = nullptr;
         b->cap = 0;
-        size_t cap = std::max<size_t>(total, 1024);
         PG_CUDA(cudaMallocHost(&b->h_desc, cap * sizeof(RowDesc)));
-        PG_CUDA(cudaMalloc(&b->d_desc, cap * sizeof(RowDesc)));
+        PG_CUDA(cudaMallocAsync(&b->d_desc, cap * sizeof(RowDesc), st));
         b->cap = cap;
     }
     for (const auto& k : b->plan) {
@@ -196,16 +204,23 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
     }
     PG_CUDA(cudaMemcpyAsync(b->d_desc, b->h_desc, total * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
     PG_CUDA(cudaEventRecord(b->copied, st));
-    if (!use_graph) return enqueue(b, st);
+    if (!use_graph) {
+        int rc = enqueue(b, st);
+        if (rc) return rc;
+        PG_CUDA(cudaEventRecord(b->finished, st));
+        return PG_OK;
+    }
     if (b->exec && same_plan(b->plan, b->graph_plan) && b->graph_desc == b->d_desc) {
         PG_CUDA(cudaGraphLaunch(b->exec, st));
         count_launch(2 * b->plan.size());
+        PG_CUDA(cudaEventRecord(b->finished, st));
         return PG_OK;
     }
     // first call of this shape: run it directly (this also performs each kernel's
     // one-time attribute setup outside any capture), then capture it for replay
     int rc = enqueue(b, st);
     if (rc) return rc;
+    PG_CUDA(cudaEventRecord(b->finished, st));
     destroy_graph(b);
     cudaStream_t cap;
     PG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));

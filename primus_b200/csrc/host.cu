@@ -209,6 +209,44 @@ int build_host_table(uint32_t log_n, uint64_t q, HostNttTable& t) {
     return PG_OK;
 }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+// the device's scratch pool, created on first use (NULL if creation failed)
+cudaMemPool_t scratch_pool(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
+}
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = scratch_pool(dev);
+    if (!pool) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+cudaError_t scratch_free(void* p, cudaStream_t st) { return cudaFreeAsync(p, st); }
+
 }  // namespace pg
 
 using namespace pg;
@@ -237,6 +275,15 @@ const char* pg_last_error(void) { return t_last_error.c_str(); }
 const char* pg_version(void) { return "primus_b200 0.1 (sm_100a)"; }
 
 uint64_t pg_launch_count(void) { return g_launches.load(); }
+
+int pg_scratch_trim(size_t keep_bytes) {
+    int dev = 0;
+    PG_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool = scratch_pool(dev);
+    if (!pool) return set_error(PG_ERR_CUDA, "scratch pool unavailable");
+    PG_CUDA(cudaMemPoolTrimTo(pool, keep_bytes));
+    return PG_OK;
+}
 
 int pg_device_count(int* count) {
     if (!count) return set_error(PG_ERR_INVALID_ARGUMENT, "count is NULL");

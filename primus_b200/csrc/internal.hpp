@@ -20,6 +20,13 @@ void clear_error();
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// ---- scratch: stream-ordered allocations from a library-owned pool per device
+// that keeps freed memory (release threshold = unlimited), so a call that needs
+// scratch does not map fresh memory after every synchronize
+cudaMemPool_t scratch_pool(int dev);
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+cudaError_t scratch_free(void* p, cudaStream_t st);
+
 #define PG_CUDA(expr)                                              \
     do {                                                           \
         cudaError_t _e = (expr);                                   \

@@ -125,7 +125,7 @@ struct Workspace {
     bool owned = false;
     cudaStream_t st = 0;
     ~Workspace() {
-        if (owned && ptr) cudaFreeAsync(ptr, st);
+        if (owned && ptr) scratch_free(ptr, st);
     }
 };
 
@@ -136,7 +136,7 @@ int get_workspace(Workspace& w, void* given, size_t given_bytes, size_t need, cu
         w.ptr = given;
         return PG_OK;
     }
-    cudaError_t e = cudaMallocAsync(&w.ptr, need, st);
+    cudaError_t e = scratch_alloc(&w.ptr, need, st);
     if (e != cudaSuccess) return cuda_status(e, "workspace allocation");
     w.owned = true;
     return PG_OK;

@@ -150,14 +150,14 @@ static int launch_pw(const pg_ntt_table* t, uint64_t* x, const uint64_t* y, cons
         if (!h_scalars) return set_error(PG_ERR_INVALID_ARGUMENT, "scalars is NULL");
         for (uint32_t l = 0; l < t->L; ++l)
             if (h_scalars[l] >= t->moduli[l]) return set_error(PG_ERR_INVALID_ARGUMENT, "scalar not below its modulus");
-        PG_CUDA(cudaMallocAsync(&d_sc, t->L * sizeof(uint64_t), st));
+        PG_CUDA(scratch_alloc((void**)&d_sc, t->L * sizeof(uint64_t), st));
         PG_CUDA(cudaMemcpyAsync(d_sc, h_scalars, t->L * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         a.scalars = d_sc;
     }
     pw_kernel<OP><<<grid_for(a.pairs), 256, 0, st>>>(a);
     count_launch();
     cudaError_t e = cudaGetLastError();
-    if (d_sc) cudaFreeAsync(d_sc, st);
+    if (d_sc) scratch_free(d_sc, st);
     if (e != cudaSuccess) return cuda_status(e, "pointwise kernel launch");
     return PG_OK;
 }

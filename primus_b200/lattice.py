@@ -137,6 +137,10 @@ def ext_product_workspace_size(table, basis: GadgetBasis, k: int, batch: int) ->
     return int(nat.lib().pg_ext_product_workspace_size(table.h, basis.h, k, batch))
 
 
+def key_switch_workspace_size(table, basis: GadgetBasis, k_in: int, k_out: int, batch: int) -> int:
+    return int(nat.lib().pg_key_switch_workspace_size(table.h, basis.h, k_in, k_out, batch))
+
+
 def glev_mac_crt_poly(table, basis: GadgetBasis, k: int, acc: DeviceBuffer, glev: DeviceBuffer,
                       crt_poly: DeviceBuffer, stream=None):
     call("pg_glev_mac_crt_poly", table.h, basis.h, k, acc.ptr, glev.ptr, crt_poly.ptr, None, 0, _sh(stream))

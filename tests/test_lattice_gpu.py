@@ -143,6 +143,12 @@ def test_external_product_bit_exact(gpu, log_n, L, k, lb, batch):
     dout2 = gpu.DeviceBuffer(glwe.size)
     gpu.external_product(table, g, k, din, dk, dout2, batch, workspace=ws)
     assert np.array_equal(dout2.numpy(), exp)
+    # the library's scratch pool, trimmed to nothing, is refilled on the next call
+    from primus_b200 import _native as nat
+    nat.call("pg_scratch_trim", 0)
+    dout3 = gpu.DeviceBuffer(glwe.size)
+    gpu.external_product(table, g, k, din, dk, dout3, batch)
+    assert np.array_equal(dout3.numpy(), exp)
 
 
 def test_external_product_decrypts(gpu):
