@@ -425,8 +425,21 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
     ws = P.DeviceBuffer(P.ext_product_workspace_size(tab, g, k, batch) // 8 + 1)
     ms = _time_stream(P, stream, lambda: P.external_product(tab, g, k, glwe, ggsw, out, batch, workspace=ws,
                                                             stream=stream), 10)
+    ms_coeff = _time_stream(P, stream, lambda: P.external_product_coeff(tab, g, k, glwe, ggsw, out, batch,
+                                                                        workspace=ws, stream=stream), 10)
+    # butterflies per ciphertext: (k+1)*d forward + (k+1) inverse NTTs of N/2 * log2 N
+    bfly_fwd = (k + 1) * g.d * (n // 2) * 11
+    bfly_all = bfly_fwd + (k + 1) * (n // 2) * 11
+    io_bytes = batch * (k + 1) * n * 8 * 2 + ggsw.count * 8
     res = {"workload": "GLWE x GGSW external product, N=2048, q < 2^54, B = 2^7, d = 7, k = 1, 4096 ciphertexts",
-           "ms_per_batch": ms, "ext_products_per_s": batch / (ms / 1e3)}
+           "kernel": "ext_fused_kernel (decompose -> NTT -> MAC [-> INTT] in one launch, one CTA per ciphertext)",
+           "ms_per_batch": ms, "ext_products_per_s": batch / (ms / 1e3),
+           "ntt_domain_out": {"ms_per_batch": ms, "ext_products_per_s": batch / (ms / 1e3),
+                              "g_butterflies_per_s": batch * bfly_fwd / (ms / 1e3) / 1e9,
+                              "hbm_gbs": io_bytes / (ms / 1e3) / 1e9},
+           "coeff_out_with_intt": {"ms_per_batch": ms_coeff, "ext_products_per_s": batch / (ms_coeff / 1e3),
+                                   "g_butterflies_per_s": batch * bfly_all / (ms_coeff / 1e3) / 1e9,
+                                   "hbm_gbs": io_bytes / (ms_coeff / 1e3) / 1e9}}
     if cpu:
         import oracle as O
         t0 = time.perf_counter()
@@ -434,7 +447,7 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
         ob = O.RnsBase([q])
         og = O.GadgetBasis(ob, 7)
         lat = O.Lattice(ot, ob, og)
-        sample = 256
+        sample = 2048
         gg = O.uniform(1, 1, q, (k + 1) * og.d * (k + 1) * n)
         ct = O.uniform(2, 2, q, sample * (k + 1) * n)
         t0 = time.perf_counter()

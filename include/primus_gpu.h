@@ -259,7 +259,7 @@ int pg_gadget_decompose_lift(const pg_gadget_basis *basis, const uint64_t *d_val
  * Key and GGSW operands are in the NTT domain; outputs are canonical NTT-domain
  * residues.  The table's moduli must equal the basis's RNS base.  Scratch:
  * pass d_workspace of at least *_workspace_size() bytes, or NULL to let the
- * call take stream-ordered scratch (cudaMallocAsync) and release it. */
+ * call take stream-ordered scratch from the library's pool (pg_scratch_trim). */
 /* batch GLWE (CRT/coefficient form, [batch][k+1][L][N]) x one GGSW -> GLWE
  * (NTT domain, [batch][k+1][L][N]); CrtGlwe::mul_dcrt_ggsw_inplace
  * (primus_lattice/src/glwe/crt.rs:202-229) */
@@ -268,6 +268,15 @@ size_t pg_ext_product_workspace_size(const pg_ntt_table *table, const pg_gadget_
 int pg_ext_product(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
                    const uint64_t *d_glwe_in, const uint64_t *d_ggsw, uint64_t *d_glwe_out,
                    size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
+/* The external product followed by inverse_transform_slice of every output
+ * poly (primus_ntt/src/ntt/primitive.rs:246-296): the GLWE comes back in
+ * coefficient form, the shape of a blind-rotation accumulator step.  For k = 1,
+ * one prime, single-word gadget values and N = 2^10..2^12 the whole step
+ * (decompose -> NTT -> MAC -> INTT) is one kernel; pg_ext_product uses the same
+ * kernel without the inverse for those shapes.  Workspace as pg_ext_product. */
+int pg_ext_product_coeff(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                         const uint64_t *d_glwe_in, const uint64_t *d_ggsw, uint64_t *d_glwe_out,
+                         size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
 /* acc ([k+1][L][N], NTT domain) += GLev x poly, the poly as CRT residues [L][N]
  * (add_dcrt_glev_mul_crt_poly_assign, glwe/dcrt.rs:170-247) or as BigUints
  * [N][W] (add_dcrt_glev_mul_big_uint_poly_assign, glwe/dcrt.rs:249-325) */

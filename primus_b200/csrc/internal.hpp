@@ -112,6 +112,28 @@ struct NttArgs {
 
 enum NttMode { MODE_FWD = 0, MODE_INV = 1, MODE_RT = 2 };
 
+// one gadget digit's window in the BigUint value: bits [shr, ...) of limb
+// `index`, continued by `mask1` bits of limb index + 1 when the digit straddles
+struct DigitMask {
+    uint32_t index, shr, shl, pad;
+    uint64_t mask0, mask1;
+};
+
+// gadget decomposition parameters of a basis whose values fit one word (W = 1)
+struct GadgetWord {
+    uint64_t bm1, carry_mask, basis, split, npq, init_mask;
+    int has_split, has_init;
+    uint32_t d, log_basis;
+    const DigitMask* masks;  // device [d]
+};
+
+// fused GLWE x GGSW external product for single-prime, single-word shapes
+// (k = 1): decomposition, forward NTT of every digit row, MAC and optionally the
+// inverse NTT of the outputs in one kernel, one CTA per ciphertext
+bool ext_fused_eligible(const pg_ntt_table* t, const GadgetWord& gw, uint32_t k);
+int launch_ext_fused(const pg_ntt_table* t, const GadgetWord& gw, const uint64_t* in, const uint64_t* key,
+                     uint64_t* out, size_t batch, bool out_coeff, cudaStream_t st);
+
 inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, int lazy) {
     NttArgs a{};
     a.data = data;

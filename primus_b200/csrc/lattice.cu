@@ -29,6 +29,7 @@ uint32_t rns_W(const pg_rns_base* b);
 const uint64_t* rns_moduli(const pg_rns_base* b);
 const pg_rns_base* gadget_base(const pg_gadget_basis* g);
 uint32_t gadget_d(const pg_gadget_basis* g);
+bool gadget_word(const pg_gadget_basis* g, GadgetWord* out);
 int launch_compose(const pg_rns_base* b, const uint64_t* res, uint64_t* out, size_t count, size_t n, uint32_t ppg,
                    size_t group_stride, cudaStream_t st);
 int launch_gadget(const pg_gadget_basis* g, const uint64_t* vals, uint64_t* out, size_t count, size_t n, bool lift,
@@ -192,6 +193,29 @@ int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t*
 }
 
 
+// GLWE x GGSW for a batch: the fused one-kernel form where the shape allows it
+// (k = 1, one prime, single-word values, N = 2^10..2^12), else the pipeline of
+// compose -> lifted digits -> batched NTT -> MAC (-> inverse NTT of the outputs)
+int ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
+                const uint64_t* d_ggsw, uint64_t* d_out, size_t batch, void* d_ws, size_t ws_size, cudaStream_t st,
+                bool out_coeff) {
+    GadgetWord gw;
+    // the fused kernel reads key rows and writes outputs with 16-byte vector accesses
+    const bool aligned = ((uintptr_t)d_ggsw % 16 == 0) && ((uintptr_t)d_out % 16 == 0);
+    if (aligned && gadget_word(g, &gw) && ext_fused_eligible(t, gw, k))
+        return launch_ext_fused(t, gw, d_in, d_ggsw, d_out, batch, out_coeff, st);
+    const size_t polys = batch * (k + 1);
+    Workspace w;
+    int rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, 0), st);
+    if (rc) return rc;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, d_in, true, polys, k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)w.ptr, &dig, st);
+    if (rc) return rc;
+    rc = launch_mac(t, gadget_d(g), d_out, nullptr, nullptr, d_ggsw, dig, batch, k + 1, k + 1, 0, st);
+    if (rc || !out_coeff) return rc;
+    return launch_ntt(make_args(t, d_out, polys * t->L, 0), t->log_n, MODE_INV, st);
+}
+
 // ---------------------------------------------------------------------------
 // External product without any device allocation.
 //
@@ -243,15 +267,17 @@ int pg_ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, 
     if (rc) return rc;
     if (batch == 0) return PG_OK;
     if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
-    cudaStream_t st = (cudaStream_t)stream;
-    const size_t polys = batch * (k + 1);
-    Workspace w;
-    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, 0), st);
+    return ext_product(t, g, k, d_in, d_ggsw, d_out, batch, d_ws, ws_size, (cudaStream_t)stream, false);
+}
+
+int pg_ext_product_coeff(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
+                         const uint64_t* d_ggsw, uint64_t* d_out, size_t batch, void* d_ws, size_t ws_size,
+                         void* stream) {
+    int rc = check_compat(t, g);
     if (rc) return rc;
-    uint64_t* dig = nullptr;
-    rc = digits_pipeline(t, g, d_in, true, polys, k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)w.ptr, &dig, st);
-    if (rc) return rc;
-    return launch_mac(t, gadget_d(g), d_out, nullptr, nullptr, d_ggsw, dig, batch, k + 1, k + 1, 0, st);
+    if (batch == 0) return PG_OK;
+    if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    return ext_product(t, g, k, d_in, d_ggsw, d_out, batch, d_ws, ws_size, (cudaStream_t)stream, true);
 }
 
 int pg_glev_mac_crt_poly(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, uint64_t* d_acc,

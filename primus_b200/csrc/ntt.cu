@@ -538,6 +538,153 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
 
 }  // namespace pg
 
+namespace pg {
+
+// ============================================================================
+// Fused external product (GLWE x GGSW, k = 1, one prime, single-word values):
+// CrtGlwe::mul_dcrt_ggsw_inplace (primus_lattice/src/glwe/crt.rs:202-229) and,
+// for OUT_COEFF, inverse_transform_slice of both output polys.  One CTA per
+// ciphertext.  For each input poly i the CTA decomposes its coefficients into
+// d gadget digits (digits of one poly kept in shared memory), then for each
+// digit j lifts the digit row to residues mod q, runs the forward NTT in
+// shared memory and multiply-accumulates the NTT-domain row against the
+// GGSW rows key[i][j][c] into 128-bit register accumulators, one per output
+// element.  Outputs are canonical residues (NTT domain, or coefficient form
+// after the in-kernel inverse NTT): the same residues as the reference's
+// per-digit sequence, since every step is exact arithmetic mod q.
+// ============================================================================
+struct ExtFusedArgs {
+    const uint64_t* in;   // [B][2][N] coefficient form
+    const uint64_t* key;  // [2][d][2][N] NTT domain
+    uint64_t* out;        // [B][2][N]
+    const ulonglong2* fwd;
+    const ulonglong2* inv;
+    const ulonglong2* inv_n;
+    const ulonglong2* inv_last;
+    Barrett bar;
+    GadgetWord gw;
+    uint64_t B;
+    int out_coeff;
+};
+
+// d digits of one word v (init_value_carry_slice_inplace, basis.rs:307-331, and
+// unsigned_decompose, common.rs:150-160, with W = 1), written to dst[j * N]
+template <typename DT, int N>
+PG_DEV void decompose_word(uint64_t v, const GadgetWord& g, DT* dst) {
+    if (g.has_split && v >= g.split) v += g.npq;
+    uint64_t carry = g.has_init ? ((v & g.init_mask) != 0) : 0;
+    for (uint32_t j = 0; j < g.d; ++j) {
+        const DigitMask m = g.masks[j];
+        // limb 1 is the zero guard limb: only limb 0 contributes bits
+        uint64_t temp = m.index == 0 ? (v & m.mask0) >> m.shr : 0;
+        temp += carry;
+        carry = (temp & g.carry_mask) != 0;
+        dst[(size_t)j * N] = (DT)(temp & g.bm1);
+    }
+}
+
+template <int LOG_N, int LOG_E, typename DT, bool FAST>
+__global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFusedArgs a) {
+    constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E, KP = 2;
+    extern __shared__ uint64_t smem_ext[];
+    // shared memory: NTT exchange buffer | 128-bit accumulators [KP][E][T] | digits [d][N]
+    uint64_t* sm = smem_ext;
+    ulonglong2* acc = reinterpret_cast<ulonglong2*>(smem_ext + padded(N));
+    DT* dg = reinterpret_cast<DT*>(acc + KP * N);
+    const uint32_t tid = threadIdx.x;
+    const uint64_t b = blockIdx.x;
+    const Barrett bar = a.bar;
+    const uint64_t q = bar.q, q2 = q << 1, nq = 0 - q;
+    const uint32_t d = a.gw.d;
+    const uint64_t basis = a.gw.basis, half = (basis + 1) / 2, lift = q - basis;
+    using R0 = FwdRounds<LOG_N, LOG_E, 0>;
+    static_assert(R0::G == LOG_N - LOG_E, "first forward group is the column tid + jj*T");
+    // each thread owns accumulator entries (c, e, tid): no other thread touches them
+#pragma unroll
+    for (int ce = 0; ce < KP * E; ++ce) acc[ce * T + tid] = make_ulonglong2(0, 0);
+    uint32_t terms = 0;
+    for (int i = 0; i < KP; ++i) {
+        // this thread's coefficients tid + jj*T; it alone reads their digits back
+        const uint64_t* src = a.in + (b * KP + i) * N;
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) decompose_word<DT, N>(src[tid + jj * T], a.gw, dg + tid + jj * T);
+        for (uint32_t j = 0; j < d; ++j) {
+            uint64_t x[E];
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) {
+                const uint64_t v = dg[(size_t)j * N + tid + jj * T];
+                x[jj] = (basis == 2 || v < half) ? v : lift + v;  // wrapping_decompose_small_values
+            }
+            fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, a.fwd, q2, nq);
+            __syncthreads();  // the previous row's last shared-memory reads are done
+            fwd_rest<LOG_N, LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, a.fwd, q2, nq);
+            if constexpr (!FAST) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) x[e] = canon4(x[e], q, q2);
+            }
+            // x = NTT-domain elements tid*E .. tid*E+E-1 of digit row (i, j); products
+            // are below 2^122, so 8 of them plus a folded value stay below 2^128
+            const bool fold = terms == 8;
+            terms = fold ? 1 : terms + 1;
+            const uint64_t* kp = a.key + ((size_t)(i * d + j) * KP) * N + tid * E;
+#pragma unroll
+            for (int c = 0; c < KP; ++c)
+#pragma unroll
+                for (int e = 0; e < E; e += 2) {
+                    ulonglong2 w;
+                    asm("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(w.x), "=l"(w.y) : "l"(kp + c * N + e));
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        ulonglong2 s = acc[(c * E + e + h) * T + tid];
+                        if (fold) {
+                            s.x = barrett_reduce_2limb(s.x, s.y, bar);
+                            s.y = 0;
+                        }
+                        const uint64_t kv = h ? w.y : w.x;
+                        const uint64_t pl = kv * x[e + h], ph = mulhi64(kv, x[e + h]);
+                        s.x += pl;
+                        s.y += ph + (s.x < pl);
+                        acc[(c * E + e + h) * T + tid] = s;
+                    }
+                }
+        }
+    }
+    uint64_t* out = a.out + b * KP * N;
+    if (!a.out_coeff) {
+#pragma unroll
+        for (int c = 0; c < KP; ++c)
+#pragma unroll
+            for (int e = 0; e < E; e += 2) {
+                const ulonglong2 s0 = acc[(c * E + e) * T + tid], s1 = acc[(c * E + e + 1) * T + tid];
+                const uint64_t r0 = barrett_reduce_2limb(s0.x, s0.y, bar);
+                const uint64_t r1 = barrett_reduce_2limb(s1.x, s1.y, bar);
+                asm volatile("st.global.v2.u64 [%0], {%1, %2};" ::"l"(out + c * N + tid * E + e), "l"(r0), "l"(r1)
+                             : "memory");
+            }
+        return;
+    }
+    // coefficient form: inverse NTT of each output poly; the first inverse group
+    // is the contiguous tid*E .. tid*E+E-1, so the accumulators feed it directly
+    using I0 = InvRounds<LOG_N, LOG_E, 0>;
+    static_assert(I0::G == 0, "first inverse group is contiguous");
+#pragma unroll 1
+    for (int c = 0; c < KP; ++c) {
+        uint64_t x[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const ulonglong2 s = acc[(c * E + e) * T + tid];
+            x[e] = barrett_reduce_2limb(s.x, s.y, bar);
+        }
+        __syncthreads();  // earlier shared-memory reads of the exchange buffer are done
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, tid * E, 0, a.inv, a.inv_n, a.inv_last, q, nq);
+        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT>(x, sm, tid, 0, a.inv, a.inv_n, a.inv_last, q, nq);
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) out[c * N + tid + jj * T] = x[jj];
+    }
+}
+
+}  // namespace pg
+
 // ============================================================================
 // Launch dispatch
 // ============================================================================
@@ -618,6 +765,70 @@ static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
 
 // fast schedule: every modulus below 2^58 so 36q < 2^64 (see fwd_bfly_fast)
 static bool fast_ok(const NttArgs& a) { return a.max_modulus < (1ull << 58); }
+
+
+// the opt-in maximum of dynamic shared memory per CTA on sm_100 (227 KiB)
+constexpr size_t kExtFusedMaxSmem = 227 * 1024;
+
+template <int LOG_N, int LOG_E, typename DT, bool FAST>
+static int launch_ext_fused_t(const ExtFusedArgs& a, size_t smem, cudaStream_t st) {
+    constexpr int T = 1 << (LOG_N - LOG_E);
+    auto kern = ext_fused_kernel<LOG_N, LOG_E, DT, FAST>;
+    // shared memory grows with the digit count; raise the limit to the largest allowed once
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kExtFusedMaxSmem);
+    if (attr != cudaSuccess) return cuda_status(attr, "ext_fused_kernel: shared memory attribute");
+    kern<<<(unsigned)a.B, T, smem, st>>>(a);
+    count_launch();
+    PG_LAUNCH_CHECK("ext_fused_kernel launch");
+    return PG_OK;
+}
+
+template <typename DT, bool FAST>
+static int launch_ext_fused_n(const ExtFusedArgs& a, uint32_t log_n, size_t smem, cudaStream_t st) {
+    switch (log_n) {
+        case 10: return launch_ext_fused_t<10, 3, DT, FAST>(a, smem, st);
+        case 11: return launch_ext_fused_t<11, 3, DT, FAST>(a, smem, st);
+        case 12: return launch_ext_fused_t<12, 3, DT, FAST>(a, smem, st);
+        default: return set_error(PG_ERR_UNSUPPORTED, "fused external product: log_n outside 10..12");
+    }
+}
+
+static size_t ext_fused_smem(const pg_ntt_table* t, const GadgetWord& gw) {
+    const size_t dt = gw.log_basis <= 16 ? 2 : 8;
+    return (size_t)padded((int)t->n) * 8 + 2 * t->n * 16 + (size_t)gw.d * t->n * dt;
+}
+
+bool ext_fused_eligible(const pg_ntt_table* t, const GadgetWord& gw, uint32_t k) {
+    if (k != 1 || t->L != 1 || t->log_n < 10 || t->log_n > 12) return false;
+    if (gw.basis < 2 || gw.basis > t->moduli[0] || gw.d == 0) return false;
+    return ext_fused_smem(t, gw) <= kExtFusedMaxSmem;
+}
+
+int launch_ext_fused(const pg_ntt_table* t, const GadgetWord& gw, const uint64_t* in, const uint64_t* key,
+                     uint64_t* out, size_t batch, bool out_coeff, cudaStream_t st) {
+    if (batch == 0) return PG_OK;
+    if (batch > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many ciphertexts for one launch");
+    ExtFusedArgs a{};
+    a.in = in;
+    a.key = key;
+    a.out = out;
+    a.fwd = t->d_fwd;
+    a.inv = t->d_inv;
+    a.inv_n = t->d_inv_n;
+    a.inv_last = t->d_inv_last;
+    a.bar = h_barrett(t->moduli[0]);
+    a.gw = gw;
+    a.B = batch;
+    a.out_coeff = out_coeff ? 1 : 0;
+    const size_t smem = ext_fused_smem(t, gw);
+    const bool fast = t->moduli[0] < (1ull << 58);
+    if (gw.log_basis <= 16)
+        return fast ? launch_ext_fused_n<uint16_t, true>(a, t->log_n, smem, st)
+                    : launch_ext_fused_n<uint16_t, false>(a, t->log_n, smem, st);
+    return fast ? launch_ext_fused_n<uint64_t, true>(a, t->log_n, smem, st)
+                : launch_ext_fused_n<uint64_t, false>(a, t->log_n, smem, st);
+}
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
     if (a.rows == 0) return PG_OK;

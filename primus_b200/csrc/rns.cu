@@ -99,11 +99,6 @@ struct pg_rns_base {
     Barrett* d_bar = nullptr;        // [L]
 };
 
-struct DigitMask {
-    uint32_t index, shr, shl, pad;
-    uint64_t mask0, mask1;
-};
-
 struct pg_gadget_basis {
     const pg_rns_base* base = nullptr;
     uint32_t W = 0, L = 0, d = 0, log_basis = 0, drop_bits = 0;
@@ -130,6 +125,25 @@ uint32_t rns_L(const pg_rns_base* b) { return b->L; }
 uint32_t rns_W(const pg_rns_base* b) { return b->W; }
 const pg_rns_base* gadget_base(const pg_gadget_basis* g) { return g->base; }
 uint32_t gadget_d(const pg_gadget_basis* g) { return g->d; }
+// the basis as single-word parameters; false when its values need more than one word
+bool gadget_word(const pg_gadget_basis* g, GadgetWord* out) {
+    if (g->W != 1) return false;
+    GadgetWord w{};
+    w.bm1 = g->bm1;
+    w.carry_mask = g->carry_mask;
+    w.basis = g->basis;
+    w.split = g->has_split ? g->split[0] : 0;
+    w.npq = g->has_split ? g->npq[0] : 0;
+    w.init_mask = g->init_mask;
+    w.has_split = g->has_split;
+    w.has_init = g->has_init && g->init_index == 0;
+    w.d = g->d;
+    w.log_basis = g->log_basis;
+    w.masks = g->d_masks;
+    if (g->has_init && g->init_index != 0) return false;
+    *out = w;
+    return true;
+}
 const uint64_t* rns_moduli(const pg_rns_base* b) { return b->moduli.data(); }
 }  // namespace pg
 

@@ -133,6 +133,17 @@ def external_product(table, basis: GadgetBasis, k: int, glwe_in: DeviceBuffer, g
     call("pg_ext_product", table.h, basis.h, k, glwe_in.ptr, ggsw.ptr, glwe_out.ptr, batch, ws, wsb, _sh(stream))
 
 
+def external_product_coeff(table, basis: GadgetBasis, k: int, glwe_in: DeviceBuffer, ggsw: DeviceBuffer,
+                           glwe_out: DeviceBuffer, batch: int, workspace: DeviceBuffer | None = None, stream=None):
+    """external_product followed by the inverse NTT of every output poly: the
+    GLWE comes back in coefficient form (one kernel for k = 1, one prime,
+    N = 2^10..2^12)."""
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_ext_product_coeff", table.h, basis.h, k, glwe_in.ptr, ggsw.ptr, glwe_out.ptr, batch, ws, wsb,
+         _sh(stream))
+
+
 def ext_product_workspace_size(table, basis: GadgetBasis, k: int, batch: int) -> int:
     return int(nat.lib().pg_ext_product_workspace_size(table.h, basis.h, k, batch))
 
