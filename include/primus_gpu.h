@@ -312,6 +312,28 @@ int pg_ext_product_noalloc(const pg_ntt_table *table, const pg_gadget_basis *bas
                            const uint64_t *d_glwe_in, const uint64_t *d_ggsw,
                            uint64_t *d_glwe_out, size_t batch, void *stream);
 
+/* Hybrid RNS key switch with K special primes and digit groups of `alpha`
+ * consecutive Q limbs (dnum = ceil(L / alpha) groups).  No reference
+ * counterpart: the reference's key switch is the BigUint gadget form
+ * (pg_key_switch).  The table holds L + K primes, Q first then P.
+ *   for each mask a_i and group g: ModUp (a_i's D_g residues kept, every other
+ *   QP limb by fast base conversion), forward NTT, acc[c] += ext (.) key[i][g][c];
+ *   ModDown: inverse NTT of acc's P limbs, fast conversion P -> Q, forward NTT,
+ *   (acc_Q - conv) * P^-1;  c_out = -ModDown(acc) + (0, .., NTT(b)).
+ * key: [k_in][dnum][k_out+1][L+K][N] NTT domain, row [i][g] encrypting
+ * [P]_{q_l} * s_in_i on the limbs of D_g (0 elsewhere) under s_out over QP.
+ * c_in: [batch][k_in+1][L][N] coefficient form; c_out: [batch][k_out+1][L][N]
+ * NTT domain, canonical.  alpha <= 8, K <= 8. */
+typedef struct pg_hybrid_ks pg_hybrid_ks;
+int pg_hybrid_ks_create(const pg_ntt_table *table, uint32_t L, uint32_t K, uint32_t alpha,
+                        pg_hybrid_ks **out);
+int pg_hybrid_ks_destroy(pg_hybrid_ks *ks);
+uint32_t pg_hybrid_ks_dnum(const pg_hybrid_ks *ks);
+size_t pg_hybrid_ks_workspace_size(const pg_hybrid_ks *ks, uint32_t k_in, uint32_t k_out, size_t batch);
+int pg_key_switch_hybrid(const pg_hybrid_ks *ks, uint32_t k_in, uint32_t k_out, const uint64_t *d_key,
+                         const uint64_t *d_c_in, uint64_t *d_c_out, size_t batch, void *d_workspace,
+                         size_t workspace_bytes, void *stream);
+
 /* ----------------------------------------------- uneven batches of products
  * A job multiplies two coefficient-form DCRT polys of its own ring degree:
  * a <- a * b (negacyclic), b <- NTT(b), using the first moduli_count primes of

@@ -122,6 +122,11 @@ def lib():
             "orc_ksk_generate": (None, [C.c_void_p, C.c_uint32, C.c_uint32, u64p, u64p, C.c_uint64, C.c_double, u64p]),
             "orc_glwe_decrypt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, C.c_uint64, C.c_uint64, u64p]),
             "orc_bfv_delta": (None, [C.c_void_p, C.c_uint64, u64p]),
+            "orc_hybrid_ks_new": (C.c_void_p, [C.c_uint32, u64p, C.c_uint32, C.c_uint32, C.c_uint32]),
+            "orc_hybrid_ks_delete": (None, [C.c_void_p]),
+            "orc_hybrid_ks_dnum": (C.c_uint32, [C.c_void_p]),
+            "orc_hybrid_ks_factor": (None, [C.c_void_p, C.c_uint32, u64p]),
+            "orc_hybrid_key_switch": (None, [C.c_void_p, C.c_uint32, C.c_uint32, u64p, u64p, u64p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -505,4 +510,34 @@ class Lattice:
     def delta(self, t):
         out = np.zeros(self.L, np.uint64)
         lib().orc_bfv_delta(self.base.h, t, p64(out))
+        return out
+
+
+class HybridKeySwitch:
+    """Hybrid RNS key switch with K special primes and digit groups of alpha
+    limbs (a definition of this build; the reference has no such key switch).
+    moduli = Q (L primes) followed by P (K primes)."""
+
+    def __init__(self, log_n: int, moduli, L: int, K: int, alpha: int):
+        self.moduli = [int(q) for q in moduli]
+        assert len(self.moduli) == L + K
+        self.log_n, self.n, self.L, self.K, self.alpha = log_n, 1 << log_n, L, K, alpha
+        self.h = lib().orc_hybrid_ks_new(log_n, p64(u64(self.moduli)), L, K, alpha)
+        if not self.h:
+            raise ValueError("hybrid key switch parameters rejected")
+        self.dnum = int(lib().orc_hybrid_ks_dnum(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_hybrid_ks_delete(self.h)
+            self.h = None
+
+    def factor(self, g: int) -> np.ndarray:
+        out = np.zeros(self.L + self.K, np.uint64)
+        lib().orc_hybrid_ks_factor(self.h, g, p64(out))
+        return out
+
+    def key_switch(self, k_in: int, k_out: int, key, c_in) -> np.ndarray:
+        out = np.zeros((k_out + 1) * self.L * self.n, np.uint64)
+        lib().orc_hybrid_key_switch(self.h, k_in, k_out, p64(u64(key)), p64(u64(c_in)), p64(out))
         return out

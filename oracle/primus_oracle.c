@@ -1351,3 +1351,170 @@ void orc_glwe_decrypt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *sk_n
     orc_rns_base_delete(btg);
     free(ph);
 }
+
+/* ======================================================================
+ * Hybrid RNS key switch with special primes (definition in the header)
+ * ====================================================================== */
+struct orc_hybrid_ks {
+    uint32_t L, K, alpha, dnum, log_n;
+    size_t n;
+    uint64_t *moduli;            /* [L+K] */
+    orc_ntt_table **tables;      /* [L+K] */
+    orc_rns_base **gin, **gout;  /* per group: D_g, and the other QP limbs */
+    orc_base_converter **gconv;  /* per group: D_g -> others */
+    uint32_t **gout_limbs;       /* per group: limb index of each output row */
+    orc_rns_base *bp, *bq;
+    orc_base_converter *pq;      /* P -> Q */
+    uint64_t *p_inv;             /* [L] P^-1 mod q_l */
+};
+
+static uint32_t hyb_group_lo(const orc_hybrid_ks *h, uint32_t g) { return g * h->alpha; }
+static uint32_t hyb_group_hi(const orc_hybrid_ks *h, uint32_t g) {
+    uint32_t e = (g + 1) * h->alpha;
+    return e < h->L ? e : h->L;
+}
+
+void orc_hybrid_ks_delete(orc_hybrid_ks *h) {
+    if (!h) return;
+    for (uint32_t l = 0; h->tables && l < h->L + h->K; ++l) orc_ntt_table_delete(h->tables[l]);
+    for (uint32_t g = 0; g < h->dnum; ++g) {
+        if (h->gconv) orc_base_converter_delete(h->gconv[g]);
+        if (h->gin) orc_rns_base_delete(h->gin[g]);
+        if (h->gout) orc_rns_base_delete(h->gout[g]);
+        if (h->gout_limbs) free(h->gout_limbs[g]);
+    }
+    free(h->tables);
+    free(h->gconv);
+    free(h->gin);
+    free(h->gout);
+    free(h->gout_limbs);
+    if (h->pq) orc_base_converter_delete(h->pq);
+    if (h->bp) orc_rns_base_delete(h->bp);
+    if (h->bq) orc_rns_base_delete(h->bq);
+    free(h->moduli);
+    free(h->p_inv);
+    free(h);
+}
+
+orc_hybrid_ks *orc_hybrid_ks_new(uint32_t log_n, const uint64_t *moduli, uint32_t L, uint32_t K,
+                                 uint32_t alpha) {
+    if (L == 0 || K == 0 || alpha == 0 || alpha > L) return NULL;
+    orc_hybrid_ks *h = calloc(1, sizeof *h);
+    h->L = L;
+    h->K = K;
+    h->alpha = alpha;
+    h->dnum = (L + alpha - 1) / alpha;
+    h->log_n = log_n;
+    h->n = (size_t)1 << log_n;
+    const uint32_t LK = L + K;
+    h->moduli = malloc(LK * 8);
+    memcpy(h->moduli, moduli, LK * 8);
+    h->tables = calloc(LK, sizeof *h->tables);
+    for (uint32_t l = 0; l < LK; ++l)
+        if (!(h->tables[l] = orc_ntt_table_new(log_n, moduli[l]))) goto fail;
+    h->gin = calloc(h->dnum, sizeof *h->gin);
+    h->gout = calloc(h->dnum, sizeof *h->gout);
+    h->gconv = calloc(h->dnum, sizeof *h->gconv);
+    h->gout_limbs = calloc(h->dnum, sizeof *h->gout_limbs);
+    uint64_t *tmp = malloc(LK * 8);
+    for (uint32_t g = 0; g < h->dnum; ++g) {
+        const uint32_t lo = hyb_group_lo(h, g), hi = hyb_group_hi(h, g);
+        h->gin[g] = orc_rns_base_new(moduli + lo, hi - lo);
+        uint32_t m = 0;
+        h->gout_limbs[g] = malloc(LK * sizeof(uint32_t));
+        for (uint32_t l = 0; l < LK; ++l)
+            if (l < lo || l >= hi) {
+                h->gout_limbs[g][m] = l;
+                tmp[m++] = moduli[l];
+            }
+        h->gout[g] = orc_rns_base_new(tmp, m);
+        if (!h->gin[g] || !h->gout[g]) {
+            free(tmp);
+            goto fail;
+        }
+        h->gconv[g] = orc_base_converter_new(h->gin[g], h->gout[g]);
+    }
+    free(tmp);
+    h->bq = orc_rns_base_new(moduli, L);
+    h->bp = orc_rns_base_new(moduli + L, K);
+    if (!h->bq || !h->bp) goto fail;
+    h->pq = orc_base_converter_new(h->bp, h->bq);
+    h->p_inv = malloc(L * 8);
+    for (uint32_t l = 0; l < L; ++l) {
+        uint64_t pm = 1;
+        for (uint32_t k = 0; k < K; ++k) pm = orc_mulmod(pm, moduli[L + k] % moduli[l], moduli[l]);
+        h->p_inv[l] = orc_invmod(pm, moduli[l]);
+        if (h->p_inv[l] == 0) goto fail;
+    }
+    return h;
+fail:
+    orc_hybrid_ks_delete(h);
+    return NULL;
+}
+
+uint32_t orc_hybrid_ks_dnum(const orc_hybrid_ks *h) { return h->dnum; }
+
+/* P * (Q/Q_g) * ((Q/Q_g)^-1 mod Q_g) mod r: [P]_{q_l} on the limbs of D_g, 0 elsewhere */
+void orc_hybrid_ks_factor(const orc_hybrid_ks *h, uint32_t g, uint64_t *fac) {
+    const uint32_t lo = hyb_group_lo(h, g), hi = hyb_group_hi(h, g);
+    for (uint32_t l = 0; l < h->L + h->K; ++l) {
+        fac[l] = 0;
+        if (l >= lo && l < hi) {
+            uint64_t pm = 1;
+            for (uint32_t k = 0; k < h->K; ++k) pm = orc_mulmod(pm, h->moduli[h->L + k] % h->moduli[l], h->moduli[l]);
+            fac[l] = pm;
+        }
+    }
+}
+
+void orc_hybrid_key_switch(const orc_hybrid_ks *h, uint32_t k_in, uint32_t k_out, const uint64_t *key,
+                           const uint64_t *c_in, uint64_t *c_out) {
+    const size_t n = h->n;
+    const uint32_t L = h->L, K = h->K, LK = L + K, KO = k_out + 1;
+    const size_t pq = (size_t)L * n, pqp = (size_t)LK * n;
+    uint64_t *acc = calloc((size_t)KO * pqp, 8);
+    uint64_t *ext = malloc(pqp * 8);
+    uint64_t *conv = malloc(pqp * 8);
+    for (uint32_t i = 0; i < k_in; ++i) {
+        const uint64_t *a = c_in + (size_t)i * pq;
+        for (uint32_t g = 0; g < h->dnum; ++g) {
+            const uint32_t lo = hyb_group_lo(h, g), hi = hyb_group_hi(h, g);
+            /* ModUp: D_g residues kept, the other limbs by fast base conversion */
+            memcpy(ext + (size_t)lo * n, a + (size_t)lo * n, (size_t)(hi - lo) * n * 8);
+            orc_fast_convert_array(h->gconv[g], a + (size_t)lo * n, conv, n);
+            for (uint32_t m = 0; m < h->gout[g]->L; ++m)
+                memcpy(ext + (size_t)h->gout_limbs[g][m] * n, conv + (size_t)m * n, n * 8);
+            for (uint32_t l = 0; l < LK; ++l) orc_ntt_forward(h->tables[l], ext + (size_t)l * n);
+            const uint64_t *row = key + ((size_t)i * h->dnum + g) * KO * pqp;
+            for (uint32_t c = 0; c < KO; ++c)
+                for (uint32_t l = 0; l < LK; ++l)
+                    orc_add_mul_assign(acc + (size_t)c * pqp + (size_t)l * n, ext + (size_t)l * n,
+                                       row + (size_t)c * pqp + (size_t)l * n, n, h->moduli[l]);
+        }
+    }
+    /* b of the input, in the NTT domain */
+    uint64_t *bt = malloc(pq * 8);
+    memcpy(bt, c_in + (size_t)k_in * pq, pq * 8);
+    for (uint32_t l = 0; l < L; ++l) orc_ntt_forward(h->tables[l], bt + (size_t)l * n);
+    for (uint32_t c = 0; c < KO; ++c) {
+        uint64_t *ac = acc + (size_t)c * pqp;
+        /* ModDown: P limbs to coefficients, fast-convert to Q, back to NTT */
+        for (uint32_t k = 0; k < K; ++k) orc_ntt_inverse(h->tables[L + k], ac + (size_t)(L + k) * n);
+        orc_fast_convert_array(h->pq, ac + (size_t)L * n, conv, n);
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint64_t q = h->moduli[l];
+            uint64_t *cv = conv + (size_t)l * n;
+            orc_ntt_forward(h->tables[l], cv);
+            uint64_t *o = c_out + (size_t)c * pq + (size_t)l * n;
+            memcpy(o, ac + (size_t)l * n, n * 8);
+            orc_sub_assign(o, cv, n, q);
+            orc_mul_scalar_assign(o, h->p_inv[l], n, q);
+            orc_neg_assign(o, n, q);
+            if (c == k_out) orc_add_assign(o, bt + (size_t)l * n, n, q);
+        }
+    }
+    free(bt);
+    free(acc);
+    free(ext);
+    free(conv);
+}

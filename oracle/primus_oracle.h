@@ -264,6 +264,29 @@ void orc_glwe_decrypt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *sk_n
 /* delta = round(Q/t) mod each q_i (parameter/glwe.rs:332-338) */
 void orc_bfv_delta(const orc_rns_base *base, uint64_t t, uint64_t *delta_res);
 
+/* ---- hybrid RNS key switch with special primes (no reference counterpart:
+ * the reference's key switch is the BigUint gadget form above).  Definition:
+ * moduli = Q (L primes) then P (K special primes); digit groups D_g are the
+ * consecutive Q limbs [g*alpha, min(L, (g+1)*alpha)).  For each input a_i
+ * (coefficient form over Q) and group g, ModUp fast-converts a_i's D_g residues
+ * to every other limb of QP (fast_convert_array semantics), keeping D_g's own
+ * residues; the extended poly is NTT'd limb by limb and multiply-accumulated
+ * with key row [i][g] ([k_in][dnum][k_out+1][L+K][N], NTT domain; the row
+ * encrypts P * (Q/Q_g) * ((Q/Q_g)^-1 mod Q_g) * s_in_i under s_out over QP).
+ * ModDown of each accumulated poly: inverse NTT of its P limbs, fast
+ * conversion P -> Q, NTT, then (acc_Q - conv) * P^-1 mod q_l.  The output is
+ * c_out = -ModDown(sum) + (0, .., NTT(b)) over Q in the NTT domain, as the
+ * BigUint key switch (key_switch.rs:96-127). */
+typedef struct orc_hybrid_ks orc_hybrid_ks;
+orc_hybrid_ks *orc_hybrid_ks_new(uint32_t log_n, const uint64_t *moduli, uint32_t L, uint32_t K,
+                                 uint32_t alpha);
+void orc_hybrid_ks_delete(orc_hybrid_ks *h);
+uint32_t orc_hybrid_ks_dnum(const orc_hybrid_ks *h);
+/* the key-row message factor of group g, as residues over QP ([L+K]) */
+void orc_hybrid_ks_factor(const orc_hybrid_ks *h, uint32_t g, uint64_t *fac);
+void orc_hybrid_key_switch(const orc_hybrid_ks *h, uint32_t k_in, uint32_t k_out, const uint64_t *key,
+                           const uint64_t *c_in, uint64_t *c_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,420 @@
+// Hybrid RNS key switch with special primes.
+//
+// The reference's key switch decomposes each mask poly into BigUint gadget
+// digits (primus_fhe_core/src/key_switch.rs:79-128).  This is the other standard
+// form, over a modulus chain Q (L primes) extended by K special primes P, with
+// digit groups of `alpha` consecutive Q limbs (dnum = ceil(L / alpha) groups).
+// The reference has no such path, so its definition is this build's own, stated
+// once more here:
+//
+//   for each input mask a_i (coefficient form over Q) and group g:
+//     ModUp:  ext = a_i's residues on the limbs of D_g, and on every other limb
+//             of QP the fast base conversion of those residues
+//             (fast_convert_array semantics, primus_rns/src/converter.rs:147-175)
+//     acc[c] += NTT(ext) (.) key[i][g][c]              (over QP, NTT domain)
+//   ModDown of acc[c]: inverse NTT of its P limbs, fast conversion P -> Q,
+//     forward NTT, then (acc_Q - conv) * P^-1 mod q_l
+//   c_out = -ModDown(acc) + (0, .., NTT(b))           (the reference's sign form)
+//
+// The key row [i][g] encrypts P * (Q/Q_g) * ((Q/Q_g)^-1 mod Q_g) * s_in_i under
+// s_out over QP, i.e. [P]_{q_l} * s_in_i on the limbs of D_g and 0 elsewhere.
+//
+// Launch sequence for a batch: modup_kernel -> forward NTT of every extended
+// row -> the MAC kernel (Q and P limbs written apart) -> inverse NTT of the P
+// limbs -> pconv_kernel (P -> Q) -> forward NTT of the converted rows and of b
+// -> finish_kernel.  Each step runs over the whole batch in one launch.
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "internal.hpp"
+
+using namespace pg;
+
+namespace {
+constexpr uint32_t kMaxAlpha = 8;  // residues held per thread in ModUp
+constexpr uint32_t kMaxK = 8;      // special primes held per thread in ModDown
+}  // namespace
+
+struct pg_hybrid_ks {
+    const pg_ntt_table* t = nullptr;  // L + K primes: Q then P
+    pg_ntt_table tq, tp;              // views of the Q and P limbs (no ownership)
+    uint32_t L = 0, K = 0, alpha = 0, dnum = 0;
+    ulonglong2* d_ginv = nullptr;  // [L] Shoup pair of ((Q_g/q_i)^-1 mod q_i), q_i in group g
+    uint64_t* d_gmat = nullptr;    // per group g: [L+K-alpha_g][alpha_g] (Q_g/q_i) mod r_j, at gmat_off[g]
+    uint32_t* d_gout = nullptr;    // per group g: [L+K-alpha_g] output limb indices, at gout_off[g]
+    std::vector<uint32_t> gmat_off, gout_off;
+    ulonglong2* d_pinv_k = nullptr;  // [K] Shoup pair of ((P/p_k)^-1 mod p_k)
+    uint64_t* d_pmat = nullptr;      // [L][K] (P/p_k) mod q_l
+    ulonglong2* d_pinv = nullptr;    // [L] Shoup pair of (P^-1 mod q_l)
+    uint32_t* d_offs = nullptr;      // [2 * dnum]: gmat_off then gout_off
+};
+
+namespace {
+
+struct ModUpArgs {
+    const uint64_t* in;  // [B][k_in+1][L][N]
+    uint64_t* ext;       // [B*k_in][dnum][L+K][N]
+    const ulonglong2* ginv;
+    const uint64_t* gmat;
+    const uint32_t* gout;
+    const uint32_t* gmat_off;  // [dnum]
+    const uint32_t* gout_off;  // [dnum]
+    const uint64_t* moduli;    // [L+K]
+    const Barrett* bar;        // [L+K]
+    size_t polys, N;           // polys = B * k_in
+    uint32_t k_in, L, K, alpha, dnum, log_n;
+};
+
+// one thread per (input mask, group, coefficient)
+__global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
+    const size_t total = a.polys * a.dnum * a.N;
+    const uint32_t LK = a.L + a.K;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = t & (a.N - 1);
+        const uint32_t g = (uint32_t)((t >> a.log_n) % a.dnum);
+        const size_t p = (t >> a.log_n) / a.dnum;  // b * k_in + i
+        const size_t b = p / a.k_in, i = p % a.k_in;
+        const uint64_t* src = a.in + ((b * (a.k_in + 1) + i) * a.L) * a.N + x;
+        uint64_t* dst = a.ext + ((p * a.dnum + g) * LK) * a.N + x;
+        const uint32_t lo = g * a.alpha, hi = min(a.L, lo + a.alpha), ag = hi - lo;
+        uint64_t tv[kMaxAlpha];
+#pragma unroll
+        for (uint32_t m = 0; m < kMaxAlpha; ++m) {
+            if (m < ag) {
+                const uint32_t l = lo + m;
+                const uint64_t v = src[(size_t)l * a.N];
+                dst[(size_t)l * a.N] = v;
+                const ulonglong2 f = a.ginv[l];
+                tv[m] = shoup_mul(f.x, f.y, v, a.moduli[l]);
+            }
+        }
+        const uint64_t* mat = a.gmat + a.gmat_off[g];
+        const uint32_t* outl = a.gout + a.gout_off[g];
+        for (uint32_t j = 0; j < LK - ag; ++j) {
+            const uint32_t r = outl[j];
+            uint64_t lo64 = 0, hi64 = 0;
+#pragma unroll
+            for (uint32_t m = 0; m < kMaxAlpha; ++m)
+                if (m < ag) {  // at most 8 products below 2^124: no overflow
+                    const uint64_t w = mat[(size_t)j * ag + m];
+                    const uint64_t pl = w * tv[m], ph = mulhi64(w, tv[m]);
+                    lo64 += pl;
+                    hi64 += ph + (lo64 < pl);
+                }
+            dst[(size_t)r * a.N] = barrett_reduce_2limb(lo64, hi64, a.bar[r]);
+        }
+    }
+}
+
+struct PConvArgs {
+    const uint64_t* accp;  // [PC][K][N], coefficient form
+    uint64_t* conv;        // [PC][L][N]
+    const ulonglong2* pinv_k;
+    const uint64_t* pmat;       // [L][K]
+    const uint64_t* moduli;     // [L+K]
+    const Barrett* bar;         // [L+K]
+    size_t pc, N;
+    uint32_t L, K, log_n;
+};
+
+// fast conversion of the P limbs to the Q limbs, one thread per (poly, coefficient)
+__global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
+    const size_t total = a.pc * a.N;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = t & (a.N - 1), p = t >> a.log_n;
+        uint64_t tv[kMaxK];
+#pragma unroll
+        for (uint32_t k = 0; k < kMaxK; ++k)
+            if (k < a.K) {
+                const ulonglong2 f = a.pinv_k[k];
+                tv[k] = shoup_mul(f.x, f.y, a.accp[(p * a.K + k) * a.N + x], a.moduli[a.L + k]);
+            }
+        for (uint32_t l = 0; l < a.L; ++l) {
+            uint64_t lo64 = 0, hi64 = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < kMaxK; ++k)
+                if (k < a.K) {
+                    const uint64_t w = a.pmat[(size_t)l * a.K + k];
+                    const uint64_t pl = w * tv[k], ph = mulhi64(w, tv[k]);
+                    lo64 += pl;
+                    hi64 += ph + (lo64 < pl);
+                }
+            a.conv[(p * a.L + l) * a.N + x] = barrett_reduce_2limb(lo64, hi64, a.bar[l]);
+        }
+    }
+}
+
+struct FinishArgs {
+    const uint64_t* accq;  // [B][KO][L][N]
+    const uint64_t* conv;  // [B][KO][L][N] NTT domain
+    const uint64_t* bt;    // [B][L][N] NTT(b)
+    uint64_t* out;         // [B][KO][L][N]
+    const ulonglong2* pinv;
+    const uint64_t* moduli;
+    size_t B, N;
+    uint32_t KO, L, log_n;
+};
+
+// out = (c == KO-1 ? NTT(b) : 0) - (acc_Q - conv) * P^-1
+__global__ void __launch_bounds__(256) finish_kernel(FinishArgs a) {
+    const size_t LN = (size_t)a.L * a.N;
+    const size_t total = a.B * a.KO * LN;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t lx = t % LN;
+        const uint32_t l = (uint32_t)(lx >> a.log_n);
+        const uint32_t c = (uint32_t)((t / LN) % a.KO);
+        const size_t b = t / (LN * a.KO);
+        const uint64_t q = a.moduli[l];
+        const ulonglong2 f = a.pinv[l];
+        const uint64_t v = shoup_mul(f.x, f.y, sub_mod(a.accq[t], a.conv[t], q), q);
+        const uint64_t base = (c == a.KO - 1) ? a.bt[b * LN + lx] : 0;
+        a.out[t] = sub_mod(base, v, q);
+    }
+}
+
+unsigned grid_for(size_t work, unsigned threads) {
+    const size_t cap = 148ull * 2048 / threads;
+    size_t b = (work + threads - 1) / threads;
+    return (unsigned)std::max<size_t>(1, std::min(b, cap));
+}
+
+// a table view over limbs [first, first + count) of t (device arrays shared)
+void make_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_table& v) {
+    v.log_n = t->log_n;
+    v.L = count;
+    v.n = t->n;
+    v.device = t->device;
+    v.moduli.assign(t->moduli.begin() + first, t->moduli.begin() + first + count);
+    v.d_moduli = t->d_moduli + first;
+    v.d_fwd = t->d_fwd + (size_t)first * t->n;
+    v.d_inv = t->d_inv + (size_t)first * t->n;
+    v.d_ordinal = t->d_ordinal + (size_t)first * 2 * t->n;
+    v.d_inv_n = t->d_inv_n + first;
+    v.d_inv_last = t->d_inv_last + first;
+    v.d_barrett = t->d_barrett + first;
+}
+
+template <typename T>
+cudaError_t upload(T** d, const std::vector<T>& h) {
+    cudaError_t e = cudaMalloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T));
+    if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+ulonglong2 shoup_pair(uint64_t w, uint64_t q) { return make_ulonglong2(w, h_shoup_quotient(w, q)); }
+
+// product of moduli[idx] over idx in [lo, hi) except `skip`, mod r
+uint64_t prod_except(const std::vector<uint64_t>& m, uint32_t lo, uint32_t hi, uint32_t skip, uint64_t r) {
+    uint64_t p = 1 % r;
+    for (uint32_t i = lo; i < hi; ++i)
+        if (i != skip) p = h_mulmod(p, m[i] % r, r);
+    return p;
+}
+
+// scratch words: ext | accQ | accP | conv | bt
+struct HybridWs {
+    size_t ext, accq, accp, conv, bt;
+    size_t total() const { return ext + accq + accp + conv + bt; }
+};
+
+HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t batch) {
+    const size_t n = h->t->n, KO = k_out + 1;
+    HybridWs w;
+    w.ext = batch * k_in * h->dnum * (size_t)(h->L + h->K) * n;
+    w.accq = batch * KO * h->L * n;
+    w.accp = batch * KO * h->K * n;
+    w.conv = batch * KO * h->L * n;
+    w.bt = batch * h->L * n;
+    return w;
+}
+
+struct OwnedWs {
+    void* ptr = nullptr;
+    cudaStream_t st = 0;
+    ~OwnedWs() {
+        if (ptr) scratch_free(ptr, st);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t alpha, pg_hybrid_ks** out) {
+    if (!out) return set_error(PG_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!t) return set_error(PG_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (L == 0 || K == 0 || L + K != t->L) return set_error(PG_ERR_INVALID_ARGUMENT, "table must hold L + K primes");
+    if (alpha == 0 || alpha > L || alpha > kMaxAlpha)
+        return set_error(PG_ERR_INVALID_ARGUMENT, "alpha must be in [1, min(L, 8)]");
+    if (K > kMaxK) return set_error(PG_ERR_UNSUPPORTED, "at most 8 special primes");
+    const std::vector<uint64_t>& m = t->moduli;
+    for (uint32_t i = 0; i < L + K; ++i)
+        for (uint32_t j = i + 1; j < L + K; ++j)
+            if (m[i] == m[j]) return set_error(PG_ERR_NOT_COPRIME, "moduli must be distinct primes");
+    pg_hybrid_ks* h = new (std::nothrow) pg_hybrid_ks();
+    if (!h) return set_error(PG_ERR_OUT_OF_MEMORY, "allocation failed");
+    h->t = t;
+    h->L = L;
+    h->K = K;
+    h->alpha = alpha;
+    h->dnum = (L + alpha - 1) / alpha;
+    make_view(t, 0, L, h->tq);
+    make_view(t, L, K, h->tp);
+    std::vector<ulonglong2> ginv(L), pinv_k(K), pinv(L);
+    std::vector<uint64_t> gmat, pmat((size_t)L * K);
+    std::vector<uint32_t> gout;
+    for (uint32_t g = 0; g < h->dnum; ++g) {
+        const uint32_t lo = g * alpha, hi = std::min(L, lo + alpha);
+        for (uint32_t i = lo; i < hi; ++i) ginv[i] = shoup_pair(h_invmod(prod_except(m, lo, hi, i, m[i]), m[i]), m[i]);
+        h->gmat_off.push_back((uint32_t)gmat.size());
+        h->gout_off.push_back((uint32_t)gout.size());
+        for (uint32_t r = 0; r < L + K; ++r) {
+            if (r >= lo && r < hi) continue;
+            gout.push_back(r);
+            for (uint32_t i = lo; i < hi; ++i) gmat.push_back(prod_except(m, lo, hi, i, m[r]));
+        }
+    }
+    for (uint32_t k = 0; k < K; ++k)
+        pinv_k[k] = shoup_pair(h_invmod(prod_except(m, L, L + K, L + k, m[L + k]), m[L + k]), m[L + k]);
+    for (uint32_t l = 0; l < L; ++l) {
+        for (uint32_t k = 0; k < K; ++k) pmat[(size_t)l * K + k] = prod_except(m, L, L + K, L + k, m[l]);
+        pinv[l] = shoup_pair(h_invmod(prod_except(m, L, L + K, UINT32_MAX, m[l]), m[l]), m[l]);
+    }
+    std::vector<uint32_t> offs(h->gmat_off);
+    offs.insert(offs.end(), h->gout_off.begin(), h->gout_off.end());
+    cudaError_t e = upload(&h->d_ginv, ginv);
+    if (e == cudaSuccess) e = upload(&h->d_gmat, gmat);
+    if (e == cudaSuccess) e = upload(&h->d_gout, gout);
+    if (e == cudaSuccess) e = upload(&h->d_pinv_k, pinv_k);
+    if (e == cudaSuccess) e = upload(&h->d_pmat, pmat);
+    if (e == cudaSuccess) e = upload(&h->d_pinv, pinv);
+    if (e == cudaSuccess) e = upload(&h->d_offs, offs);
+    if (e != cudaSuccess) {
+        pg_hybrid_ks_destroy(h);
+        return cuda_status(e, "pg_hybrid_ks_create: upload");
+    }
+    *out = h;
+    return PG_OK;
+}
+
+int pg_hybrid_ks_destroy(pg_hybrid_ks* h) {
+    if (!h) return PG_OK;
+    cudaFree(h->d_ginv);
+    cudaFree(h->d_gmat);
+    cudaFree(h->d_gout);
+    cudaFree(h->d_pinv_k);
+    cudaFree(h->d_pmat);
+    cudaFree(h->d_pinv);
+    cudaFree(h->d_offs);
+    delete h;
+    return PG_OK;
+}
+
+uint32_t pg_hybrid_ks_dnum(const pg_hybrid_ks* h) { return h ? h->dnum : 0; }
+
+size_t pg_hybrid_ks_workspace_size(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t batch) {
+    if (!h) return 0;
+    return hybrid_ws(h, k_in, k_out, batch).total() * sizeof(uint64_t) + 256;
+}
+
+int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, const uint64_t* d_key,
+                         const uint64_t* d_in, uint64_t* d_out, size_t batch, void* d_ws, size_t ws_size,
+                         void* stream) {
+    if (!h) return set_error(PG_ERR_INVALID_ARGUMENT, "key switch context is NULL");
+    if (batch == 0) return PG_OK;
+    if (!d_key || !d_in || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (k_in == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k_in must be at least 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    const pg_ntt_table* t = h->t;
+    const size_t n = t->n, KO = k_out + 1, L = h->L, K = h->K;
+    const HybridWs w = hybrid_ws(h, k_in, k_out, batch);
+    const size_t need = w.total() * sizeof(uint64_t);
+    OwnedWs owned;
+    uint64_t* ws = (uint64_t*)d_ws;
+    if (ws) {
+        if (ws_size < need) return set_error(PG_ERR_INVALID_ARGUMENT, "workspace too small");
+    } else {
+        owned.st = st;
+        cudaError_t e = scratch_alloc(&owned.ptr, need, st);
+        if (e != cudaSuccess) return cuda_status(e, "key switch workspace");
+        ws = (uint64_t*)owned.ptr;
+    }
+    uint64_t* ext = ws;
+    uint64_t* accq = ext + w.ext;
+    uint64_t* accp = accq + w.accq;
+    uint64_t* conv = accp + w.accp;
+    uint64_t* bt = conv + w.conv;
+    // ModUp of every mask of every ciphertext, all groups
+    ModUpArgs ma{};
+    ma.in = d_in;
+    ma.ext = ext;
+    ma.ginv = h->d_ginv;
+    ma.gmat = h->d_gmat;
+    ma.gout = h->d_gout;
+    ma.gmat_off = h->d_offs;
+    ma.gout_off = h->d_offs + h->dnum;
+    ma.moduli = t->d_moduli;
+    ma.bar = t->d_barrett;
+    ma.polys = batch * k_in;
+    ma.N = n;
+    ma.k_in = k_in;
+    ma.L = h->L;
+    ma.K = h->K;
+    ma.alpha = h->alpha;
+    ma.dnum = h->dnum;
+    ma.log_n = t->log_n;
+    modup_kernel<<<grid_for(ma.polys * h->dnum * n, 256), 256, 0, st>>>(ma);
+    count_launch();
+    PG_LAUNCH_CHECK("modup_kernel launch");
+    int rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
+    if (rc) return rc;
+    // sum over masks and groups, Q limbs to accq, P limbs to accp
+    rc = launch_mac(t, h->dnum, accq, nullptr, nullptr, d_key, ext, batch, k_in, (uint32_t)KO, 0, st, accp,
+                    h->L);
+    if (rc) return rc;
+    // ModDown: P limbs to coefficients, convert to Q, back to the NTT domain
+    rc = launch_ntt(make_args(&h->tp, accp, batch * KO * K, 0), t->log_n, MODE_INV, st);
+    if (rc) return rc;
+    PConvArgs pa{};
+    pa.accp = accp;
+    pa.conv = conv;
+    pa.pinv_k = h->d_pinv_k;
+    pa.pmat = h->d_pmat;
+    pa.moduli = t->d_moduli;
+    pa.bar = t->d_barrett;
+    pa.pc = batch * KO;
+    pa.N = n;
+    pa.L = h->L;
+    pa.K = h->K;
+    pa.log_n = t->log_n;
+    pconv_kernel<<<grid_for(pa.pc * n, 256), 256, 0, st>>>(pa);
+    count_launch();
+    PG_LAUNCH_CHECK("pconv_kernel launch");
+    rc = launch_ntt(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, MODE_FWD, st);
+    if (rc) return rc;
+    // b of every input, moved to the NTT domain
+    PG_CUDA(cudaMemcpy2DAsync(bt, L * n * 8, d_in + (size_t)k_in * L * n, (size_t)(k_in + 1) * L * n * 8, L * n * 8,
+                              batch, cudaMemcpyDeviceToDevice, st));
+    rc = launch_ntt(make_args(&h->tq, bt, batch * L, 0), t->log_n, MODE_FWD, st);
+    if (rc) return rc;
+    FinishArgs fa{};
+    fa.accq = accq;
+    fa.conv = conv;
+    fa.bt = bt;
+    fa.out = d_out;
+    fa.pinv = h->d_pinv;
+    fa.moduli = t->d_moduli;
+    fa.B = batch;
+    fa.N = n;
+    fa.KO = (uint32_t)KO;
+    fa.L = h->L;
+    fa.log_n = t->log_n;
+    finish_kernel<<<grid_for(batch * KO * L * n, 256), 256, 0, st>>>(fa);
+    count_launch();
+    PG_LAUNCH_CHECK("finish_kernel launch");
+    return PG_OK;
+}
+
+}  // extern "C"

@@ -155,4 +155,13 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
 }
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
+
+// out[b][c] = base + sign * sum_{i < kin, j < d} key[i][j][c] (.) dig[b][i][j] over the
+// table's L limbs (NTT domain, canonical); base = acc (accumulate) or, with
+// negate, add_last on the last output poly.  With out_hi, limbs >= l_split are
+// written to out_hi as [B][kout][L - l_split][N] and the rest to out as
+// [B][kout][l_split][N].
+int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t* acc, const uint64_t* add_last,
+               const uint64_t* key, const uint64_t* dig, size_t B, uint32_t kin, uint32_t kout, int negate,
+               cudaStream_t st, uint64_t* out_hi = nullptr, uint32_t l_split = 0);
 }  // namespace pg

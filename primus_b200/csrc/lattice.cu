@@ -56,8 +56,9 @@ struct MacArgs {
     const uint64_t* key;       // [KIN][d][KOUT][L][N]
     const uint64_t* dig;       // [B][KIN][d][L][N]
     const Barrett* bar;        // [L]
+    uint64_t* out_hi;          // optional: limbs >= l_split go to [B][KOUT][L - l_split][N] here
     size_t B, N;
-    uint32_t KIN, KOUT, d, L, log_n;
+    uint32_t KIN, KOUT, d, L, log_n, l_split;
     int negate;
 };
 
@@ -92,7 +93,16 @@ __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
             uint64_t base = a.acc ? a.acc[t] : 0;
             r = add_mod(base, s, m.q);
         }
-        a.out[t] = r;
+        if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+            const size_t bc = t / LN;
+            const size_t x = lx & (a.N - 1);
+            if (l < a.l_split)
+                a.out[(bc * a.l_split + l) * a.N + x] = r;
+            else
+                a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
+        } else {
+            a.out[t] = r;
+        }
     }
 }
 
@@ -167,10 +177,14 @@ int digits_pipeline(const pg_ntt_table* t, const pg_gadget_basis* g, const uint6
     return PG_OK;
 }
 
-int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t* acc, const uint64_t* add_last,
-               const uint64_t* key, const uint64_t* dig, size_t B, uint32_t kin, uint32_t kout, int negate,
-               cudaStream_t st) {
+}  // namespace
+
+int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t* acc, const uint64_t* add_last,
+                   const uint64_t* key, const uint64_t* dig, size_t B, uint32_t kin, uint32_t kout, int negate,
+                   cudaStream_t st, uint64_t* out_hi, uint32_t l_split) {
     MacArgs a{};
+    a.out_hi = out_hi;
+    a.l_split = l_split;
     a.out = out;
     a.acc = acc;
     a.add_last = add_last;
@@ -191,6 +205,8 @@ int launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t*
     PG_LAUNCH_CHECK("mac_kernel launch");
     return PG_OK;
 }
+
+namespace {
 
 
 // GLWE x GGSW for a batch: the fused one-kernel form where the shape allows it

@@ -167,3 +167,36 @@ def key_switch(table, basis: GadgetBasis, k_in: int, k_out: int, key: DeviceBuff
     ws = workspace.ptr if workspace is not None else None
     wsb = workspace.count * 8 if workspace is not None else 0
     call("pg_key_switch", table.h, basis.h, k_in, k_out, key.ptr, c_in.ptr, c_out.ptr, batch, ws, wsb, _sh(stream))
+
+
+class HybridKeySwitch:
+    """Hybrid RNS key switch over a table of L + K primes (Q then P) with digit
+    groups of `alpha` Q limbs (pg_hybrid_ks_*).  No reference counterpart."""
+
+    def __init__(self, table, L: int, K: int, alpha: int):
+        h = C.c_void_p()
+        call("pg_hybrid_ks_create", table.h, L, K, alpha, C.byref(h))
+        self.h = h.value
+        self.table, self.L, self.K, self.alpha = table, L, K, alpha
+        self.dnum = int(nat.lib().pg_hybrid_ks_dnum(self.h))
+
+    def workspace_size(self, k_in: int, k_out: int, batch: int) -> int:
+        return int(nat.lib().pg_hybrid_ks_workspace_size(self.h, k_in, k_out, batch))
+
+    def key_switch(self, k_in: int, k_out: int, key: DeviceBuffer, c_in: DeviceBuffer, c_out: DeviceBuffer,
+                   batch: int, workspace: DeviceBuffer | None = None, stream=None):
+        ws = workspace.ptr if workspace is not None else None
+        wsb = workspace.count * 8 if workspace is not None else 0
+        call("pg_key_switch_hybrid", self.h, k_in, k_out, key.ptr, c_in.ptr, c_out.ptr, batch, ws, wsb,
+             _sh(stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_hybrid_ks_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
