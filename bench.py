@@ -460,8 +460,8 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
 
 def bench_served(P, stream, count=2000, seed=0x5EED0005):
     """Mixed request stream: 50% RNS polymul (N = 2^12..2^16, L = 4..24), 30%
-    external product (the N = 2048 shape above), 20% key switch (N = 2^15, L = 16,
-    BigUint gadget with log_basis 49 -> 16 digits, k = 1).  The plain form runs
+    external product (the N = 2048 shape above), 20% hybrid RNS key switch
+    (N = 2^15, L = 16 plus K = 4 special primes, 4-limb digit groups, k = 1).  The plain form runs
     each request as its own synchronous call; the served form replays the same
     trace into the continuous-batching server at Poisson arrival rates."""
     rng = np.random.default_rng(seed)
@@ -473,11 +473,13 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     xg = P.GadgetBasis(P.RnsBase([xq]), 7)
     xkey = P.DeviceBuffer(2 * xg.d * 2 * 2048)
     xt.fill_uniform(xkey, 2 * xg.d * 2, seed=seed + 1, stream=stream)
-    ks_moduli = P.ntt_primes(1 << 50, 1 << 16, 16)
+    # hybrid key switch: Q = 16 primes, P = 4 special primes, 4-limb digit groups
+    ks_moduli = P.ntt_primes(1 << 50, 1 << 16, 20)
     kt = P.DcrtTable(15, ks_moduli)
-    kg = P.GadgetBasis(P.RnsBase(ks_moduli), 49)
-    kkey = P.DeviceBuffer(kg.d * 2 * 16 * 32768)
-    kt.fill_uniform(kkey, kg.d * 2, seed=seed + 2, stream=stream)
+    kq = P.DcrtTable(15, ks_moduli[:16])  # Q limbs only, for the input generator
+    hks = P.HybridKeySwitch(kt, 16, 4, 4)
+    kkey = P.DeviceBuffer(hks.dnum * 2 * 20 * 32768)
+    kt.fill_uniform(kkey, hks.dnum * 2, seed=seed + 2, stream=stream)
     kinds = rng.choice(3, size=count, p=[0.5, 0.3, 0.2])
     trace = []  # (kind, buffers...)
     for i, kd in enumerate(kinds):
@@ -494,7 +496,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
             trace.append(("xp", di, do))
         else:
             di, do = P.DeviceBuffer(2 * 16 * 32768), P.DeviceBuffer(2 * 16 * 32768)
-            kt.fill_uniform(di, 2, seed=seed + 6, stream0=32 * i, stream=stream)
+            kq.fill_uniform(di, 2, seed=seed + 6, stream0=32 * i, stream=stream)
             trace.append(("ks", di, do))
     stream.synchronize()
 
@@ -505,7 +507,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
         elif it[0] == "xp":
             P.external_product(xt, xg, 1, it[1], xkey, it[2], 1, stream=stream)
         else:
-            P.key_switch(kt, kg, 1, 1, kkey, it[1], it[2], 1, stream=stream)
+            hks.key_switch(1, 1, kkey, it[1], it[2], 1, stream=stream)
 
     for it in trace[:50]:
         plain_call(it)
@@ -543,7 +545,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     # ---- served
     srv = P.Server(memory_budget_bytes=8 << 30, slots=4, max_batch=512, polymul_tables=list(pm_tables.values()))
     xid = srv.register_key(2, xt, xg, 1, 1, xkey)
-    kid = srv.register_key(3, kt, kg, 1, 1, kkey)
+    kid = srv.register_hybrid_key(hks, 1, 1, kkey)
     reqs = []
     for it in trace:
         if it[0] == "pm":
@@ -572,11 +574,13 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
         t0 = time.perf_counter()
         lat = srv.replay(reqs, arrivals)
         served_runs.append(summary(lat, time.perf_counter() - t0, offered))
-        served_runs[-1]["mean_batch"] = srv.stats(reset=True)["mean_batch"]
+        st = srv.stats(reset=True)
+        served_runs[-1].update({k: st[k] for k in ("mean_batch", "enqueue_mean_us", "enqueue_max_us")})
     srv.close()
     best = max(r["throughput_rps"] for r in served_runs)
     return {"workload": "served mixed stream: 50% polymul N=2^12..2^16 L=4..24, 30% ext product (N=2048, k=1, "
-                        "7-bit gadget), 20% key switch (N=2^15, L=16, 49-bit gadget, 16 digits); Poisson arrivals",
+                        "7-bit gadget), 20% hybrid key switch (N=2^15, L=16 + K=4 special primes, 4-limb digit "
+                        "groups); Poisson arrivals",
             "requests": count, "plain_capacity_rps": plain_rps, "per_kind": per_kind,
             "plain": plain_runs, "served": served_runs, "served_max_rps": best,
             "served_over_plain_capacity": best / plain_rps}

@@ -271,9 +271,10 @@ int pg_ext_product(const pg_ntt_table *table, const pg_gadget_basis *basis, uint
 /* The external product followed by inverse_transform_slice of every output
  * poly (primus_ntt/src/ntt/primitive.rs:246-296): the GLWE comes back in
  * coefficient form, the shape of a blind-rotation accumulator step.  For k = 1,
- * one prime, single-word gadget values and N = 2^10..2^12 the whole step
- * (decompose -> NTT -> MAC -> INTT) is one kernel; pg_ext_product uses the same
- * kernel without the inverse for those shapes.  Workspace as pg_ext_product. */
+ * one prime, single-word gadget values, N = 2^10..2^12 and batches of at least
+ * 64 ciphertexts the whole step (decompose -> NTT -> MAC -> INTT) is one kernel;
+ * pg_ext_product uses the same kernel without the inverse for those shapes.
+ * Workspace as pg_ext_product. */
 int pg_ext_product_coeff(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
                          const uint64_t *d_glwe_in, const uint64_t *d_ggsw, uint64_t *d_glwe_out,
                          size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
@@ -356,6 +357,9 @@ typedef struct pg_polymul_batch pg_polymul_batch;
 int pg_polymul_batch_create(const pg_ntt_table *const *tables, uint32_t table_count,
                             pg_polymul_batch **out);
 int pg_polymul_batch_destroy(pg_polymul_batch *batch);
+/* make room for `rows` row descriptors (a job of L limbs takes 3L) so that later
+ * calls up to that size allocate nothing; the batch starts with 4096 */
+int pg_polymul_batch_reserve(pg_polymul_batch *batch, size_t rows);
 int pg_polymul_batch_run(pg_polymul_batch *batch, const pg_polymul_job *h_jobs, size_t count,
                          int use_graph, void *stream);
 
@@ -392,6 +396,7 @@ typedef struct pg_server_config {
 typedef struct pg_server_stats {
     uint64_t submitted, completed, rejected, batches;
     double mean_batch, p50_us, p99_us, max_us; /* latency = submit -> completion */
+    double enqueue_mean_us, enqueue_max_us;    /* host time to put one batch on its stream */
 } pg_server_stats_t;
 
 typedef struct pg_server pg_server;
@@ -407,6 +412,10 @@ int pg_server_destroy(pg_server *server);
 int pg_server_register_key(pg_server *server, int kind, const pg_ntt_table *table,
                            const pg_gadget_basis *basis, uint32_t k_in, uint32_t k_out,
                            const uint64_t *d_key, uint32_t *key_id);
+/* register a hybrid key switch key (pg_key_switch_hybrid layout) for
+ * PG_REQ_KEY_SWITCH requests; the context and key stay owned by the caller */
+int pg_server_register_hybrid_key(pg_server *server, const pg_hybrid_ks *ks, uint32_t k_in, uint32_t k_out,
+                                  const uint64_t *d_key, uint32_t *key_id);
 /* queue one request; PG_ERR_REJECTED when the queue is full or the request
  * cannot fit one slot's scratch, PG_ERR_INVALID_ARGUMENT when malformed */
 int pg_server_submit(pg_server *server, const pg_request *request, uint64_t *ticket);

@@ -117,6 +117,10 @@ int pg_polymul_batch_create(const pg_ntt_table* const* tables, uint32_t table_co
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->finished, cudaEventDisableTiming);
+    // room for 4096 rows up front, so that typical calls never allocate
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_desc, 4096 * sizeof(RowDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_desc, 4096 * sizeof(RowDesc));
+    if (e == cudaSuccess) b->cap = 4096;
     if (e != cudaSuccess) {
         pg_polymul_batch_destroy(b);
         return cuda_status(e, "pg_polymul_batch_create");
@@ -136,8 +140,25 @@ int pg_polymul_batch_destroy(pg_polymul_batch* b) {
     if (b->copied) cudaEventDestroy(b->copied);
     if (b->finished) cudaEventDestroy(b->finished);
     cudaFreeHost(b->h_desc);
-    cudaFree(b->d_desc);  // also frees stream-ordered allocations (synchronizing)
+    cudaFree(b->d_desc);
     delete b;
+    return PG_OK;
+}
+
+int pg_polymul_batch_reserve(pg_polymul_batch* b, size_t rows) {
+    if (!b) return set_error(PG_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (rows <= b->cap) return PG_OK;
+    destroy_graph(b);  // captured launches point at the old descriptor buffer
+    PG_CUDA(cudaEventSynchronize(b->copied));
+    PG_CUDA(cudaEventSynchronize(b->finished));
+    cudaFreeHost(b->h_desc);
+    cudaFree(b->d_desc);
+    b->h_desc = nullptr;
+    b->d_desc = nullptr;
+    b->cap = 0;
+    PG_CUDA(cudaMallocHost(&b->h_desc, rows * sizeof(RowDesc)));
+    PG_CUDA(cudaMalloc(&b->d_desc, rows * sizeof(RowDesc)));
+    b->cap = rows;
     return PG_OK;
 }
 
@@ -171,21 +192,10 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
     // the previous call's descriptor copy must have left the pinned buffer
     PG_CUDA(cudaEventSynchronize(b->copied));
     if (total > b->cap) {
-        // grow geometrically; the device copy is stream-ordered so that growing
-        // does not wait for work other streams have in flight
-        destroy_graph(b);  // captured launches point at the old descriptor buffer
-        const size_t cap = std::max<size_t>(std::max<size_t>(total, 2 * b->cap), 4096);
-        cudaFreeHost(b->h_desc);
-        if (b->d_desc) {
-            PG_CUDA(cudaStreamWaitEvent(st, b->finished, 0));  // the last call may have used another stream
-            PG_CUDA(cudaFreeAsync(b->d_desc, st));
-        }
-        b->h_desc = nullptr;
-        b->d_desc = nullptr;
-        b->cap = 0;
-        PG_CUDA(cudaMallocHost(&b->h_desc, cap * sizeof(RowDesc)));
-        PG_CUDA(cudaMallocAsync(&b->d_desc, cap * sizeof(RowDesc), st));
-        b->cap = cap;
+        // grow geometrically (rare: the batch starts with room for 4096 rows and
+        // callers can reserve more); freeing waits for launches still reading
+        int rc = pg_polymul_batch_reserve(b, std::max<size_t>(total, 2 * b->cap));
+        if (rc) return rc;
     }
     for (const auto& k : b->plan) {
         const size_t n = (size_t)1 << k.log_n;

@@ -239,6 +239,9 @@ struct OwnedWs {
 
 }  // namespace
 
+uint32_t pg::hybrid_q_limbs(const pg_hybrid_ks* ks) { return ks->L; }
+size_t pg::hybrid_n(const pg_hybrid_ks* ks) { return ks->t->n; }
+
 extern "C" {
 
 int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t alpha, pg_hybrid_ks** out) {

@@ -156,6 +156,10 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
 
+// hybrid key switch context accessors (Q limb count, ring degree)
+uint32_t hybrid_q_limbs(const pg_hybrid_ks* ks);
+size_t hybrid_n(const pg_hybrid_ks* ks);
+
 // out[b][c] = base + sign * sum_{i < kin, j < d} key[i][j][c] (.) dig[b][i][j] over the
 // table's L limbs (NTT domain, canonical); base = acc (accumulate) or, with
 // negate, add_last on the last output poly.  With out_hi, limbs >= l_split are

@@ -62,46 +62,70 @@ struct MacArgs {
     int negate;
 };
 
+// One thread per (batch chunk, output poly c, limb l, coefficient x): each key
+// element is loaded once per chunk of kMacChunk ciphertexts and multiplied into
+// every ciphertext's accumulator of the chunk, so a batch reads the key
+// ceil(B / kMacChunk) times instead of B times.
+constexpr uint32_t kMacChunk = 8;
+
 __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
     const size_t LN = (size_t)a.L * a.N;
-    const size_t total = a.B * a.KOUT * LN;
+    const size_t chunks = (a.B + kMacChunk - 1) / kMacChunk;
+    const size_t total = chunks * a.KOUT * LN;
+    const size_t kstride = (size_t)a.KOUT * LN;
+    const size_t dstride = (size_t)a.KIN * a.d * LN;  // one ciphertext's digits
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t lx = t % LN;                 // l * N + x
+        const size_t lx = t % LN;  // l * N + x
         const uint32_t c = (uint32_t)((t / LN) % a.KOUT);
-        const size_t b = t / (LN * a.KOUT);
+        const size_t b0 = (t / (LN * a.KOUT)) * kMacChunk;
+        const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
         const uint32_t l = (uint32_t)(lx >> a.log_n);
         const Barrett m = a.bar[l];
-        uint64_t lo = 0, hi = 0;
+        uint64_t lo[kMacChunk], hi[kMacChunk];
+#pragma unroll
+        for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[bb] = hi[bb] = 0;
         uint32_t terms = 0;
         const uint64_t* kp = a.key + (size_t)c * LN + lx;
-        const uint64_t* dp = a.dig + b * a.KIN * a.d * LN + lx;
-        const size_t kstride = (size_t)a.KOUT * LN;
+        const uint64_t* dp = a.dig + b0 * dstride + lx;
         for (uint32_t ij = 0; ij < a.KIN * a.d; ++ij) {
-            mac128(lo, hi, __ldg(kp + ij * kstride), __ldg(dp + ij * LN));
-            if (++terms == 8) {  // products < 2^124: fold before the sum can reach 2^128
-                lo = barrett_reduce_2limb(lo, hi, m);
-                hi = 0;
+            if (terms == 8) {  // products < 2^124: fold before the sum can reach 2^128
+#pragma unroll
+                for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                    lo[bb] = barrett_reduce_2limb(lo[bb], hi[bb], m);
+                    hi[bb] = 0;
+                }
                 terms = 1;
             }
+            const uint64_t kv = __ldg(kp + ij * kstride);
+#pragma unroll
+            for (uint32_t bb = 0; bb < kMacChunk; ++bb)
+                if (bb < nb) mac128(lo[bb], hi[bb], kv, __ldg(dp + bb * dstride + ij * LN));
+            ++terms;
         }
-        uint64_t s = barrett_reduce_2limb(lo, hi, m);
-        uint64_t r;
-        if (a.negate) {
-            uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
-            r = sub_mod(base, s, m.q);
-        } else {
-            uint64_t base = a.acc ? a.acc[t] : 0;
-            r = add_mod(base, s, m.q);
-        }
-        if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
-            const size_t bc = t / LN;
-            const size_t x = lx & (a.N - 1);
-            if (l < a.l_split)
-                a.out[(bc * a.l_split + l) * a.N + x] = r;
-            else
-                a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
-        } else {
-            a.out[t] = r;
+#pragma unroll
+        for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+            if (bb >= nb) break;
+            const size_t b = b0 + bb;
+            const size_t o = (b * a.KOUT + c) * LN + lx;  // [B][KOUT][L][N] index
+            const uint64_t s = barrett_reduce_2limb(lo[bb], hi[bb], m);
+            uint64_t r;
+            if (a.negate) {
+                const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
+                r = sub_mod(base, s, m.q);
+            } else {
+                const uint64_t base = a.acc ? a.acc[o] : 0;
+                r = add_mod(base, s, m.q);
+            }
+            if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+                const size_t bc = b * a.KOUT + c;
+                const size_t x = lx & (a.N - 1);
+                if (l < a.l_split)
+                    a.out[(bc * a.l_split + l) * a.N + x] = r;
+                else
+                    a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
+            } else {
+                a.out[o] = r;
+            }
         }
     }
 }
@@ -199,7 +223,7 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     a.L = t->L;
     a.log_n = t->log_n;
     a.negate = negate;
-    const size_t total = B * kout * (size_t)t->L * t->n;
+    const size_t total = ((B + kMacChunk - 1) / kMacChunk) * kout * (size_t)t->L * t->n;
     mac_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
     count_launch();
     PG_LAUNCH_CHECK("mac_kernel launch");
@@ -208,6 +232,8 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
 
 namespace {
 
+
+constexpr size_t kExtFusedMinBatch = 64;
 
 // GLWE x GGSW for a batch: the fused one-kernel form where the shape allows it
 // (k = 1, one prime, single-word values, N = 2^10..2^12), else the pipeline of
@@ -218,7 +244,9 @@ int ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, con
     GadgetWord gw;
     // the fused kernel reads key rows and writes outputs with 16-byte vector accesses
     const bool aligned = ((uintptr_t)d_ggsw % 16 == 0) && ((uintptr_t)d_out % 16 == 0);
-    if (aligned && gadget_word(g, &gw) && ext_fused_eligible(t, gw, k))
+    // one CTA per ciphertext: small batches leave most SMs idle, and the
+    // pipeline's per-digit parallelism finishes them sooner
+    if (batch >= kExtFusedMinBatch && aligned && gadget_word(g, &gw) && ext_fused_eligible(t, gw, k))
         return launch_ext_fused(t, gw, d_in, d_ggsw, d_out, batch, out_coeff, st);
     const size_t polys = batch * (k + 1);
     Workspace w;

@@ -52,7 +52,8 @@ __global__ void gather_kernel(uint64_t* const* ptrs, uint64_t* contig, size_t wo
 struct Key {
     int kind;  // PG_REQ_EXT_PRODUCT or PG_REQ_KEY_SWITCH
     const pg_ntt_table* table;
-    const pg_gadget_basis* basis;
+    const pg_gadget_basis* basis;  // NULL for a hybrid key switch key
+    const pg_hybrid_ks* hks;       // hybrid key switch context, or NULL
     uint32_t k_in, k_out;
     const uint64_t* d_key;
     size_t in_words, out_words;
@@ -105,6 +106,7 @@ struct pg_server {
     int device = 0;
     // statistics
     uint64_t submitted = 0, completed = 0, rejected = 0, batches = 0, batched_requests = 0;
+    double enqueue_total_us = 0, enqueue_max_us = 0;
     std::vector<double> latencies;
     std::string worker_error;
 };
@@ -137,6 +139,7 @@ size_t request_scratch(const pg_server* srv, const pg_request& r) {
     const Key& k = srv->keys[r.key];
     const size_t io = (k.in_words + k.out_words) * sizeof(uint64_t);
     if (k.kind == PG_REQ_EXT_PRODUCT) return io + pg_ext_product_workspace_size(k.table, k.basis, k.k_in, 1);
+    if (k.hks) return io + pg_hybrid_ks_workspace_size(k.hks, k.k_in, k.k_out, 1);
     return io + pg_key_switch_workspace_size(k.table, k.basis, k.k_in, k.k_out, 1);
 }
 
@@ -196,6 +199,8 @@ int run_batch(pg_server* srv, Slot& s, const std::vector<Req>& batch) {
     if (rc) return rc;
     if (k.kind == PG_REQ_EXT_PRODUCT)
         rc = pg_ext_product(k.table, k.basis, k.k_in, in, k.d_key, out, n, ws, ws_bytes, s.stream);
+    else if (k.hks)
+        rc = pg_key_switch_hybrid(k.hks, k.k_in, k.k_out, k.d_key, in, out, n, ws, ws_bytes, s.stream);
     else
         rc = pg_key_switch(k.table, k.basis, k.k_in, k.k_out, k.d_key, in, out, n, ws, ws_bytes, s.stream);
     if (rc) return rc;
@@ -247,12 +252,14 @@ void worker_loop(pg_server* srv) {
         ++srv->batches;
         srv->batched_requests += batch.size();
         lock.unlock();
+        const double t_enq = now_us();
         int rc = run_batch(srv, *slot, batch);
         slot->status = rc;
         if (rc == PG_OK) {
             cudaError_t e = cudaLaunchHostFunc(slot->stream, on_batch_done, slot);
             if (e != cudaSuccess) rc = cuda_status(e, "cudaLaunchHostFunc");
         }
+        const double enq = now_us() - t_enq;
         if (rc != PG_OK) {
             // the batch never reached the GPU: fail its requests now
             slot->status = rc;
@@ -264,6 +271,8 @@ void worker_loop(pg_server* srv) {
             on_batch_done(slot);
         }
         lock.lock();
+        srv->enqueue_total_us += enq;
+        srv->enqueue_max_us = std::max(srv->enqueue_max_us, enq);
     }
 }
 
@@ -296,12 +305,18 @@ int pg_server_create(const pg_server_config* cfg, const pg_ntt_table* const* pol
             return cuda_status(e, "pg_server_create: slot");
         }
         s.scratch_bytes = share;
-        if (table_count) {
-            int rc = pg_polymul_batch_create(polymul_tables, table_count, &s.polymul);
-            if (rc) {
-                pg_server_destroy(srv);
-                return rc;
-            }
+        // everything a batch needs on the host side is allocated here, so that
+        // forming batches never allocates (allocations synchronize the device)
+        int rc = ensure_ptrs(s, 2 * (size_t)srv->cfg.max_batch);
+        if (rc == PG_OK && table_count) {
+            rc = pg_polymul_batch_create(polymul_tables, table_count, &s.polymul);
+            uint32_t max_l = 0;
+            for (uint32_t t = 0; t < table_count; ++t) max_l = std::max(max_l, polymul_tables[t]->L);
+            if (rc == PG_OK) rc = pg_polymul_batch_reserve(s.polymul, 3 * (size_t)max_l * srv->cfg.max_batch);
+        }
+        if (rc) {
+            pg_server_destroy(srv);
+            return rc;
         }
     }
     srv->tickets.reserve(1 << 16);
@@ -346,6 +361,25 @@ int pg_server_register_key(pg_server* srv, int kind, const pg_ntt_table* table, 
     const size_t LN = (size_t)table->L * table->n;
     k.in_words = (size_t)(k_in + 1) * LN;
     k.out_words = (size_t)(k.k_out + 1) * LN;
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->keys.push_back(k);
+    *key_id = (uint32_t)(srv->keys.size() - 1);
+    return PG_OK;
+}
+
+int pg_server_register_hybrid_key(pg_server* srv, const pg_hybrid_ks* ks, uint32_t k_in, uint32_t k_out,
+                                  const uint64_t* d_key, uint32_t* key_id) {
+    if (!srv || !ks || !d_key || !key_id) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (k_in == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k_in must be at least 1");
+    Key k{};
+    k.kind = PG_REQ_KEY_SWITCH;
+    k.hks = ks;
+    k.k_in = k_in;
+    k.k_out = k_out;
+    k.d_key = d_key;
+    const size_t LN = (size_t)hybrid_q_limbs(ks) * hybrid_n(ks);
+    k.in_words = (size_t)(k_in + 1) * LN;
+    k.out_words = (size_t)(k_out + 1) * LN;
     std::lock_guard<std::mutex> lock(srv->mu);
     srv->keys.push_back(k);
     *key_id = (uint32_t)(srv->keys.size() - 1);
@@ -434,7 +468,10 @@ int pg_server_stats(pg_server* srv, pg_server_stats_t* out, int reset) {
     out->p50_us = pct(0.50);
     out->p99_us = pct(0.99);
     out->max_us = l.empty() ? 0.0 : l.back();
+    out->enqueue_mean_us = srv->batches ? srv->enqueue_total_us / srv->batches : 0.0;
+    out->enqueue_max_us = srv->enqueue_max_us;
     if (reset) {
+        srv->enqueue_total_us = srv->enqueue_max_us = 0;
         srv->submitted = srv->completed = srv->rejected = srv->batches = srv->batched_requests = 0;
         srv->latencies.clear();
     }

@@ -24,7 +24,8 @@ class ServerConfig(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
                 ("batches", C.c_uint64), ("mean_batch", C.c_double), ("p50_us", C.c_double),
-                ("p99_us", C.c_double), ("max_us", C.c_double)]
+                ("p99_us", C.c_double), ("max_us", C.c_double), ("enqueue_mean_us", C.c_double),
+                ("enqueue_max_us", C.c_double)]
 
 
 def polymul_request(a, b, log_n, moduli_count):
@@ -53,6 +54,13 @@ class Server:
         kid = C.c_uint32()
         call("pg_server_register_key", self.h, kind, table.h, basis.h, k_in, k_out, d_key.ptr, C.byref(kid))
         self._keys.append((table, basis, d_key))  # keep them alive
+        return kid.value
+
+    def register_hybrid_key(self, ks, k_in, k_out, d_key):
+        """Key for PG_REQ_KEY_SWITCH requests run by the hybrid key switch `ks`."""
+        kid = C.c_uint32()
+        call("pg_server_register_hybrid_key", self.h, ks.h, k_in, k_out, d_key.ptr, C.byref(kid))
+        self._keys.append((ks, d_key))
         return kid.value
 
     def submit(self, req: Request) -> int:

@@ -1,5 +1,5 @@
 """The one-kernel external product (k = 1, one prime, single-word gadget values,
-N = 2^10..2^12): decomposition, forward NTT of every digit row, MAC and, for the
+N = 2^10..2^12, batches of 64 ciphertexts or more): decomposition, forward NTT of every digit row, MAC and, for the
 coefficient-form entry point, the inverse NTT of both outputs, all inside one
 CTA per ciphertext.  Every output is compared bit for bit with the oracle's
 CrtGlwe::mul_dcrt_ggsw_inplace (primus_lattice/src/glwe/crt.rs:202-229) and,
@@ -21,8 +21,9 @@ def _setup(log_n, q, lb):
 # (log_n, modulus bound, log_basis, batch): the blind-rotation shape (2^11, q < 2^54,
 # 7-bit digits), 16-bit digits, wide digits kept as 64-bit words, a modulus above
 # 2^58 (lazy Harvey forward schedule), and base 2 (many digits, many folds)
-SHAPES = [(11, 1 << 54, 7, 37), (10, 1 << 54, 7, 5), (12, 1 << 50, 10, 3), (11, 1 << 50, 16, 4),
-          (11, 1 << 54, 20, 3), (11, 1 << 61, 16, 3), (10, 1 << 40, 1, 2)]
+# (the fused kernel runs for batches of 64 and more; the batch of 5 takes the pipeline)
+SHAPES = [(11, 1 << 54, 7, 100), (10, 1 << 54, 7, 5), (10, 1 << 54, 7, 64), (12, 1 << 50, 10, 65),
+          (11, 1 << 50, 16, 64), (11, 1 << 54, 20, 70), (11, 1 << 61, 16, 64), (10, 1 << 40, 1, 64)]
 
 
 @pytest.mark.parametrize("log_n,bound,lb,batch", SHAPES)
@@ -81,15 +82,18 @@ def test_fused_blind_rotation_steps_decrypt(gpu):
     sk_ntt = lat.table.forward(sk)
     msg = O.uniform(41, 1, t, n)
     ct = lat.encrypt(k, sk_ntt, lat.base.wrapping_decompose_small(msg, t), lat.delta(t), 9)
-    cur = gpu.DeviceBuffer.from_numpy(lat.table.inverse(ct))
-    nxt = gpu.DeviceBuffer(ct.size)
+    # 64 copies of the ciphertext so that the one-kernel form runs
+    cur = gpu.DeviceBuffer.from_numpy(np.tile(lat.table.inverse(ct), 64))
+    nxt = gpu.DeviceBuffer(64 * ct.size)
     total = 0
     for step, deg in enumerate((5, 300, 1000)):
         dk = gpu.DeviceBuffer.from_numpy(lat.ggsw_monomial(k, sk_ntt, [1], deg, 700 + step))
-        gpu.external_product_coeff(table, g, k, cur, dk, nxt, 1)
+        gpu.external_product_coeff(table, g, k, cur, dk, nxt, 64)
         cur, nxt = nxt, cur
         total += deg
-    m = lat.decrypt(k, sk_ntt, lat.table.forward(cur.numpy()), t, 257)  # small gamma: one 54-bit prime
+    res = cur.numpy().reshape(64, -1)
+    assert (res == res[0]).all()
+    m = lat.decrypt(k, sk_ntt, lat.table.forward(res[0].copy()), t, 257)  # small gamma: one 54-bit prime
     exp = np.roll(msg.astype(np.int64), total)
     exp[:total] = (t - exp[:total]) % t
     assert np.array_equal(m, exp.astype(np.uint64))

@@ -200,3 +200,27 @@ def test_replay_reports_latencies(gpu, env):
     P.external_product(env["xt"], env["xg"], 1, di, env["xk"], want, 1)
     assert all(np.array_equal(o.numpy(), want.numpy()) for o in outs)
     srv.close()
+
+
+def test_hybrid_key_requests(gpu, env):
+    # hybrid key switch keys in the server: every result equals the plain call
+    P = gpu
+    log_n, L, K, alpha = 10, 4, 2, 2
+    n = 1 << log_n
+    moduli = O.ntt_primes(1 << 50, 2 * n, L + K)
+    table = P.DcrtTable(log_n, moduli)
+    hks = P.HybridKeySwitch(table, L, K, alpha)
+    key = np.concatenate([O.uniform_rns(21, 9 * r, moduli, n).ravel() for r in range(hks.dnum * 2)])
+    dk = P.DeviceBuffer.from_numpy(key)
+    srv, xid, _ = make_server(P, env)
+    hid = srv.register_hybrid_key(hks, 1, 1, dk)
+    ins = [O.uniform_rns(30 + i, 0, moduli[:L], 2 * n) for i in range(24)]
+    bufs = [(P.DeviceBuffer.from_numpy(x), P.DeviceBuffer(2 * L * n)) for x in ins]
+    tickets = [srv.submit(P.key_switch_request(hid, di, do)) for di, do in bufs]
+    for t in tickets:
+        srv.wait(t, timeout_us=30_000_000)
+    for (di, do) in bufs:
+        alone = P.DeviceBuffer(2 * L * n)
+        hks.key_switch(1, 1, dk, di, alone, 1)
+        assert np.array_equal(do.numpy(), alone.numpy())
+    srv.close()
