@@ -41,22 +41,30 @@ struct pg_hybrid_ks {
     pg_ntt_table tq, tp;              // views of the Q and P limbs (no ownership)
     uint32_t L = 0, K = 0, alpha = 0, dnum = 0;
     ulonglong2* d_ginv = nullptr;  // [L] Shoup pair of ((Q_g/q_i)^-1 mod q_i), q_i in group g
-    uint64_t* d_gmat = nullptr;    // per group g: [L+K-alpha_g][alpha_g] (Q_g/q_i) mod r_j, at gmat_off[g]
+    ulonglong2* d_gmat = nullptr;  // per group g: [L+K-alpha_g][alpha_g] Shoup pair of (Q_g/q_i) mod r_j, at gmat_off[g]
     uint32_t* d_gout = nullptr;    // per group g: [L+K-alpha_g] output limb indices, at gout_off[g]
     std::vector<uint32_t> gmat_off, gout_off;
     ulonglong2* d_pinv_k = nullptr;  // [K] Shoup pair of ((P/p_k)^-1 mod p_k)
-    uint64_t* d_pmat = nullptr;      // [L][K] (P/p_k) mod q_l
+    ulonglong2* d_pmat = nullptr;    // [L][K] Shoup pair of (P/p_k) mod q_l
     ulonglong2* d_pinv = nullptr;    // [L] Shoup pair of (P^-1 mod q_l)
     uint32_t* d_offs = nullptr;      // [2 * dnum]: gmat_off then gout_off
 };
 
 namespace {
 
+// v mod q for v < 16 q
+PG_DEV uint64_t reduce_below_16q(uint64_t v, uint64_t q) {
+    v = v >= 8 * q ? v - 8 * q : v;
+    v = v >= 4 * q ? v - 4 * q : v;
+    v = v >= 2 * q ? v - 2 * q : v;
+    return v >= q ? v - q : v;
+}
+
 struct ModUpArgs {
     const uint64_t* in;  // [B][k_in+1][L][N]
     uint64_t* ext;       // [B*k_in][dnum][L+K][N]
     const ulonglong2* ginv;
-    const uint64_t* gmat;
+    const ulonglong2* gmat;
     const uint32_t* gout;
     const uint32_t* gmat_off;  // [dnum]
     const uint32_t* gout_off;  // [dnum]
@@ -66,43 +74,48 @@ struct ModUpArgs {
     uint32_t k_in, L, K, alpha, dnum, log_n;
 };
 
-// one thread per (input mask, group, coefficient)
+// one thread per (input mask, group, coefficient); grid y = mask * dnum + group.
+// AMAX bounds the group size (registers held per thread).
+template <uint32_t AMAX>
 __global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
-    const size_t total = a.polys * a.dnum * a.N;
     const uint32_t LK = a.L + a.K;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t x = t & (a.N - 1);
-        const uint32_t g = (uint32_t)((t >> a.log_n) % a.dnum);
-        const size_t p = (t >> a.log_n) / a.dnum;  // b * k_in + i
+    const size_t outer = a.polys * a.dnum;
+    for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const uint32_t g = (uint32_t)(o % a.dnum);
+        const size_t p = o / a.dnum;  // b * k_in + i
         const size_t b = p / a.k_in, i = p % a.k_in;
-        const uint64_t* src = a.in + ((b * (a.k_in + 1) + i) * a.L) * a.N + x;
-        uint64_t* dst = a.ext + ((p * a.dnum + g) * LK) * a.N + x;
+        const uint64_t* src0 = a.in + ((b * (a.k_in + 1) + i) * a.L) * a.N;
+        uint64_t* dst0 = a.ext + (o * LK) * a.N;
         const uint32_t lo = g * a.alpha, hi = min(a.L, lo + a.alpha), ag = hi - lo;
-        uint64_t tv[kMaxAlpha];
-#pragma unroll
-        for (uint32_t m = 0; m < kMaxAlpha; ++m) {
-            if (m < ag) {
-                const uint32_t l = lo + m;
-                const uint64_t v = src[(size_t)l * a.N];
-                dst[(size_t)l * a.N] = v;
-                const ulonglong2 f = a.ginv[l];
-                tv[m] = shoup_mul(f.x, f.y, v, a.moduli[l]);
-            }
-        }
-        const uint64_t* mat = a.gmat + a.gmat_off[g];
+        const ulonglong2* mat = a.gmat + a.gmat_off[g];
         const uint32_t* outl = a.gout + a.gout_off[g];
-        for (uint32_t j = 0; j < LK - ag; ++j) {
-            const uint32_t r = outl[j];
-            uint64_t lo64 = 0, hi64 = 0;
+        for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.N; x += gridDim.x * blockDim.x) {
+            const uint64_t* src = src0 + x;
+            uint64_t* dst = dst0 + x;
+            uint64_t tv[AMAX];
 #pragma unroll
-            for (uint32_t m = 0; m < kMaxAlpha; ++m)
-                if (m < ag) {  // at most 8 products below 2^124: no overflow
-                    const uint64_t w = mat[(size_t)j * ag + m];
-                    const uint64_t pl = w * tv[m], ph = mulhi64(w, tv[m]);
-                    lo64 += pl;
-                    hi64 += ph + (lo64 < pl);
+            for (uint32_t m = 0; m < AMAX; ++m) {
+                tv[m] = 0;
+                if (m < ag) {
+                    const uint32_t l = lo + m;
+                    const uint64_t v = src[(size_t)l * a.N];
+                    dst[(size_t)l * a.N] = v;
+                    const ulonglong2 f = a.ginv[l];
+                    tv[m] = shoup_mul(f.x, f.y, v, a.moduli[l]);
                 }
-            dst[(size_t)r * a.N] = barrett_reduce_2limb(lo64, hi64, a.bar[r]);
+            }
+            for (uint32_t j = 0; j < LK - ag; ++j) {
+                const uint32_t r = outl[j];
+                const uint64_t rq = a.moduli[r];
+                uint64_t y = 0;  // sum of at most 8 lazy products in [0, 2 r): below 16 r < 2^64
+#pragma unroll
+                for (uint32_t m = 0; m < AMAX; ++m)
+                    if (m < ag) {
+                        const ulonglong2 w = mat[j * ag + m];
+                        y += shoup_lazy(w.x, w.y, tv[m], rq);
+                    }
+                dst[(size_t)r * a.N] = reduce_below_16q(y, rq);
+            }
         }
     }
 }
@@ -111,36 +124,40 @@ struct PConvArgs {
     const uint64_t* accp;  // [PC][K][N], coefficient form
     uint64_t* conv;        // [PC][L][N]
     const ulonglong2* pinv_k;
-    const uint64_t* pmat;       // [L][K]
+    const ulonglong2* pmat;     // [L][K]
     const uint64_t* moduli;     // [L+K]
     const Barrett* bar;         // [L+K]
     size_t pc, N;
     uint32_t L, K, log_n;
 };
 
-// fast conversion of the P limbs to the Q limbs, one thread per (poly, coefficient)
+// fast conversion of the P limbs to the Q limbs, one thread per (poly, coefficient); grid y = poly.
+// KMAX bounds the special prime count (registers held per thread).
+template <uint32_t KMAX>
 __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
-    const size_t total = a.pc * a.N;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t x = t & (a.N - 1), p = t >> a.log_n;
-        uint64_t tv[kMaxK];
+    for (size_t p = blockIdx.y; p < a.pc; p += gridDim.y) {
+        for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.N; x += gridDim.x * blockDim.x) {
+            uint64_t tv[KMAX];
 #pragma unroll
-        for (uint32_t k = 0; k < kMaxK; ++k)
-            if (k < a.K) {
-                const ulonglong2 f = a.pinv_k[k];
-                tv[k] = shoup_mul(f.x, f.y, a.accp[(p * a.K + k) * a.N + x], a.moduli[a.L + k]);
-            }
-        for (uint32_t l = 0; l < a.L; ++l) {
-            uint64_t lo64 = 0, hi64 = 0;
-#pragma unroll
-            for (uint32_t k = 0; k < kMaxK; ++k)
+            for (uint32_t k = 0; k < KMAX; ++k) {
+                tv[k] = 0;
                 if (k < a.K) {
-                    const uint64_t w = a.pmat[(size_t)l * a.K + k];
-                    const uint64_t pl = w * tv[k], ph = mulhi64(w, tv[k]);
-                    lo64 += pl;
-                    hi64 += ph + (lo64 < pl);
+                    const ulonglong2 f = a.pinv_k[k];
+                    tv[k] = shoup_mul(f.x, f.y, a.accp[(p * a.K + k) * a.N + x], a.moduli[a.L + k]);
                 }
-            a.conv[(p * a.L + l) * a.N + x] = barrett_reduce_2limb(lo64, hi64, a.bar[l]);
+            }
+            uint64_t* dst = a.conv + (p * a.L) * a.N + x;
+            for (uint32_t l = 0; l < a.L; ++l) {
+                const uint64_t ql = a.moduli[l];
+                uint64_t y = 0;  // sum of at most 8 lazy products in [0, 2 q_l): below 16 q_l < 2^64
+#pragma unroll
+                for (uint32_t k = 0; k < KMAX; ++k)
+                    if (k < a.K) {
+                        const ulonglong2 w = a.pmat[l * a.K + k];
+                        y += shoup_lazy(w.x, w.y, tv[k], ql);
+                    }
+                dst[(size_t)l * a.N] = reduce_below_16q(y, ql);
+            }
         }
     }
 }
@@ -156,28 +173,35 @@ struct FinishArgs {
     uint32_t KO, L, log_n;
 };
 
-// out = (c == KO-1 ? NTT(b) : 0) - (acc_Q - conv) * P^-1
+// out = (c == KO-1 ? NTT(b) : 0) - (acc_Q - conv) * P^-1; grid y = b * KO + c
 __global__ void __launch_bounds__(256) finish_kernel(FinishArgs a) {
-    const size_t LN = (size_t)a.L * a.N;
-    const size_t total = a.B * a.KO * LN;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t lx = t % LN;
-        const uint32_t l = (uint32_t)(lx >> a.log_n);
-        const uint32_t c = (uint32_t)((t / LN) % a.KO);
-        const size_t b = t / (LN * a.KO);
-        const uint64_t q = a.moduli[l];
-        const ulonglong2 f = a.pinv[l];
-        const uint64_t v = shoup_mul(f.x, f.y, sub_mod(a.accq[t], a.conv[t], q), q);
-        const uint64_t base = (c == a.KO - 1) ? a.bt[b * LN + lx] : 0;
-        a.out[t] = sub_mod(base, v, q);
+    const uint32_t LN = a.L * (uint32_t)a.N;
+    const size_t outer = a.B * a.KO;
+    for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const bool last = (o % a.KO) == a.KO - 1;
+        const size_t b = o / a.KO;
+        const uint64_t* aq = a.accq + o * LN;
+        const uint64_t* cv = a.conv + o * LN;
+        const uint64_t* bt = a.bt + b * LN;
+        uint64_t* out = a.out + o * LN;
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
+            const uint32_t l = lx >> a.log_n;
+            const uint64_t q = a.moduli[l];
+            const ulonglong2 f = a.pinv[l];
+            const uint64_t v = shoup_mul(f.x, f.y, sub_mod(aq[lx], cv[lx], q), q);
+            out[lx] = sub_mod(last ? bt[lx] : 0, v, q);
+        }
     }
 }
 
-unsigned grid_for(size_t work, unsigned threads) {
-    const size_t cap = 148ull * 2048 / threads;
-    size_t b = (work + threads - 1) / threads;
-    return (unsigned)std::max<size_t>(1, std::min(b, cap));
+// grid for a kernel whose x dimension covers `inner` elements with 256 threads
+// and whose y dimension covers `outer` rows (both loop when capped)
+dim3 grid2(size_t inner, size_t outer) {
+    const size_t bx = std::min<size_t>((inner + 255) / 256, 4096);
+    const size_t by = std::min<size_t>(outer, 65535);
+    return dim3((unsigned)std::max<size_t>(bx, 1), (unsigned)std::max<size_t>(by, 1));
 }
+
 
 // a table view over limbs [first, first + count) of t (device arrays shared)
 void make_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_table& v) {
@@ -254,6 +278,8 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
     if (K > kMaxK) return set_error(PG_ERR_UNSUPPORTED, "at most 8 special primes");
     const std::vector<uint64_t>& m = t->moduli;
     for (uint32_t i = 0; i < L + K; ++i)
+        if (m[i] >= (1ull << 59)) return set_error(PG_ERR_UNSUPPORTED, "hybrid key switch moduli must be below 2^59");
+    for (uint32_t i = 0; i < L + K; ++i)
         for (uint32_t j = i + 1; j < L + K; ++j)
             if (m[i] == m[j]) return set_error(PG_ERR_NOT_COPRIME, "moduli must be distinct primes");
     pg_hybrid_ks* h = new (std::nothrow) pg_hybrid_ks();
@@ -266,7 +292,7 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
     make_view(t, 0, L, h->tq);
     make_view(t, L, K, h->tp);
     std::vector<ulonglong2> ginv(L), pinv_k(K), pinv(L);
-    std::vector<uint64_t> gmat, pmat((size_t)L * K);
+    std::vector<ulonglong2> gmat, pmat((size_t)L * K);
     std::vector<uint32_t> gout;
     for (uint32_t g = 0; g < h->dnum; ++g) {
         const uint32_t lo = g * alpha, hi = std::min(L, lo + alpha);
@@ -276,13 +302,13 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
         for (uint32_t r = 0; r < L + K; ++r) {
             if (r >= lo && r < hi) continue;
             gout.push_back(r);
-            for (uint32_t i = lo; i < hi; ++i) gmat.push_back(prod_except(m, lo, hi, i, m[r]));
+            for (uint32_t i = lo; i < hi; ++i) gmat.push_back(shoup_pair(prod_except(m, lo, hi, i, m[r]), m[r]));
         }
     }
     for (uint32_t k = 0; k < K; ++k)
         pinv_k[k] = shoup_pair(h_invmod(prod_except(m, L, L + K, L + k, m[L + k]), m[L + k]), m[L + k]);
     for (uint32_t l = 0; l < L; ++l) {
-        for (uint32_t k = 0; k < K; ++k) pmat[(size_t)l * K + k] = prod_except(m, L, L + K, L + k, m[l]);
+        for (uint32_t k = 0; k < K; ++k) pmat[(size_t)l * K + k] = shoup_pair(prod_except(m, L, L + K, L + k, m[l]), m[l]);
         pinv[l] = shoup_pair(h_invmod(prod_except(m, L, L + K, UINT32_MAX, m[l]), m[l]), m[l]);
     }
     std::vector<uint32_t> offs(h->gmat_off);
@@ -368,7 +394,10 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     ma.alpha = h->alpha;
     ma.dnum = h->dnum;
     ma.log_n = t->log_n;
-    modup_kernel<<<grid_for(ma.polys * h->dnum * n, 256), 256, 0, st>>>(ma);
+    if (h->alpha <= 4)
+        modup_kernel<4><<<grid2(n, ma.polys * h->dnum), 256, 0, st>>>(ma);
+    else
+        modup_kernel<kMaxAlpha><<<grid2(n, ma.polys * h->dnum), 256, 0, st>>>(ma);
     count_launch();
     PG_LAUNCH_CHECK("modup_kernel launch");
     int rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
@@ -392,7 +421,10 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     pa.L = h->L;
     pa.K = h->K;
     pa.log_n = t->log_n;
-    pconv_kernel<<<grid_for(pa.pc * n, 256), 256, 0, st>>>(pa);
+    if (h->K <= 4)
+        pconv_kernel<4><<<grid2(n, pa.pc), 256, 0, st>>>(pa);
+    else
+        pconv_kernel<kMaxK><<<grid2(n, pa.pc), 256, 0, st>>>(pa);
     count_launch();
     PG_LAUNCH_CHECK("pconv_kernel launch");
     rc = launch_ntt(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, MODE_FWD, st);
@@ -414,7 +446,8 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     fa.KO = (uint32_t)KO;
     fa.L = h->L;
     fa.log_n = t->log_n;
-    finish_kernel<<<grid_for(batch * KO * L * n, 256), 256, 0, st>>>(fa);
+    if (L * n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
+    finish_kernel<<<grid2(L * n, batch * KO), 256, 0, st>>>(fa);
     count_launch();
     PG_LAUNCH_CHECK("finish_kernel launch");
     return PG_OK;

@@ -65,66 +65,69 @@ struct MacArgs {
 // One thread per (batch chunk, output poly c, limb l, coefficient x): each key
 // element is loaded once per chunk of kMacChunk ciphertexts and multiplied into
 // every ciphertext's accumulator of the chunk, so a batch reads the key
-// ceil(B / kMacChunk) times instead of B times.
-constexpr uint32_t kMacChunk = 8;
+// ceil(B / kMacChunk) times instead of B times.  Grid: x over the L*N
+// coefficients of a poly (32-bit index), y over (chunk, c), so that no thread
+// divides 64-bit indices.
+constexpr uint32_t kMacChunk = 4;
 
-__global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
-    const size_t LN = (size_t)a.L * a.N;
-    const size_t chunks = (a.B + kMacChunk - 1) / kMacChunk;
-    const size_t total = chunks * a.KOUT * LN;
+template <bool FOLD>
+__global__ void __launch_bounds__(256, 2) mac_kernel(MacArgs a) {
+    const uint32_t LN = a.L * (uint32_t)a.N;
+    const size_t outer = ((a.B + kMacChunk - 1) / kMacChunk) * a.KOUT;
     const size_t kstride = (size_t)a.KOUT * LN;
     const size_t dstride = (size_t)a.KIN * a.d * LN;  // one ciphertext's digits
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const size_t lx = t % LN;  // l * N + x
-        const uint32_t c = (uint32_t)((t / LN) % a.KOUT);
-        const size_t b0 = (t / (LN * a.KOUT)) * kMacChunk;
+    const uint32_t nterms = a.KIN * a.d;
+    for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const uint32_t c = (uint32_t)(o % a.KOUT);
+        const size_t b0 = (o / a.KOUT) * kMacChunk;
         const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
-        const uint32_t l = (uint32_t)(lx >> a.log_n);
-        const Barrett m = a.bar[l];
-        uint64_t lo[kMacChunk], hi[kMacChunk];
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
+            const uint32_t l = lx >> a.log_n;
+            const Barrett m = a.bar[l];
+            uint64_t lo[kMacChunk], hi[kMacChunk];
 #pragma unroll
-        for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[bb] = hi[bb] = 0;
-        uint32_t terms = 0;
-        const uint64_t* kp = a.key + (size_t)c * LN + lx;
-        const uint64_t* dp = a.dig + b0 * dstride + lx;
-        for (uint32_t ij = 0; ij < a.KIN * a.d; ++ij) {
-            if (terms == 8) {  // products < 2^124: fold before the sum can reach 2^128
+            for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[bb] = hi[bb] = 0;
+            const uint64_t* kp = a.key + (size_t)c * LN + lx;
+            const uint64_t* dp = a.dig + b0 * dstride + lx;
+#pragma unroll 2
+            for (uint32_t ij = 0; ij < nterms; ++ij) {
+                if (FOLD && ij && (ij & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
 #pragma unroll
-                for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-                    lo[bb] = barrett_reduce_2limb(lo[bb], hi[bb], m);
-                    hi[bb] = 0;
+                    for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                        lo[bb] = barrett_reduce_2limb(lo[bb], hi[bb], m);
+                        hi[bb] = 0;
+                    }
                 }
-                terms = 1;
-            }
-            const uint64_t kv = __ldg(kp + ij * kstride);
+                const uint64_t kv = __ldg(kp + ij * kstride);
+                uint64_t dv[kMacChunk];
 #pragma unroll
-            for (uint32_t bb = 0; bb < kMacChunk; ++bb)
-                if (bb < nb) mac128(lo[bb], hi[bb], kv, __ldg(dp + bb * dstride + ij * LN));
-            ++terms;
-        }
+                for (uint32_t bb = 0; bb < kMacChunk; ++bb) dv[bb] = bb < nb ? __ldg(dp + bb * dstride + ij * LN) : 0;
 #pragma unroll
-        for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-            if (bb >= nb) break;
-            const size_t b = b0 + bb;
-            const size_t o = (b * a.KOUT + c) * LN + lx;  // [B][KOUT][L][N] index
-            const uint64_t s = barrett_reduce_2limb(lo[bb], hi[bb], m);
-            uint64_t r;
-            if (a.negate) {
-                const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
-                r = sub_mod(base, s, m.q);
-            } else {
-                const uint64_t base = a.acc ? a.acc[o] : 0;
-                r = add_mod(base, s, m.q);
+                for (uint32_t bb = 0; bb < kMacChunk; ++bb) mac128(lo[bb], hi[bb], kv, dv[bb]);
             }
-            if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+#pragma unroll
+            for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                if (bb >= nb) break;
+                const size_t b = b0 + bb;
                 const size_t bc = b * a.KOUT + c;
-                const size_t x = lx & (a.N - 1);
-                if (l < a.l_split)
-                    a.out[(bc * a.l_split + l) * a.N + x] = r;
-                else
-                    a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
-            } else {
-                a.out[o] = r;
+                const uint64_t s = barrett_reduce_2limb(lo[bb], hi[bb], m);
+                uint64_t r;
+                if (a.negate) {
+                    const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
+                    r = sub_mod(base, s, m.q);
+                } else {
+                    const uint64_t base = a.acc ? a.acc[bc * LN + lx] : 0;
+                    r = add_mod(base, s, m.q);
+                }
+                if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+                    const uint32_t x = lx & ((uint32_t)a.N - 1);
+                    if (l < a.l_split)
+                        a.out[(bc * a.l_split + l) * a.N + x] = r;
+                    else
+                        a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
+                } else {
+                    a.out[bc * LN + lx] = r;
+                }
             }
         }
     }
@@ -134,6 +137,14 @@ unsigned grid_for(size_t work, unsigned threads) {
     const size_t cap = 148ull * 2048 / threads;
     size_t b = (work + threads - 1) / threads;
     return (unsigned)std::max<size_t>(1, std::min(b, cap));
+}
+
+// grid for a kernel whose x dimension covers `inner` elements with 256 threads
+// and whose y dimension covers `outer` rows (both loop when capped)
+dim3 grid2(size_t inner, size_t outer) {
+    const size_t bx = std::min<size_t>((inner + 255) / 256, 4096);
+    const size_t by = std::min<size_t>(outer, 65535);
+    return dim3((unsigned)std::max<size_t>(bx, 1), (unsigned)std::max<size_t>(by, 1));
 }
 
 int check_compat(const pg_ntt_table* t, const pg_gadget_basis* g) {
@@ -223,8 +234,12 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     a.L = t->L;
     a.log_n = t->log_n;
     a.negate = negate;
-    const size_t total = ((B + kMacChunk - 1) / kMacChunk) * kout * (size_t)t->L * t->n;
-    mac_kernel<<<grid_for(total, 256), 256, 0, st>>>(a);
+    if ((size_t)t->L * t->n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
+    const dim3 grid = grid2((size_t)t->L * t->n, ((B + kMacChunk - 1) / kMacChunk) * kout);
+    if (kin * d > 8)  // more than 8 products per output: fold the 128-bit sums every 8
+        mac_kernel<true><<<grid, 256, 0, st>>>(a);
+    else
+        mac_kernel<false><<<grid, 256, 0, st>>>(a);
     count_launch();
     PG_LAUNCH_CHECK("mac_kernel launch");
     return PG_OK;

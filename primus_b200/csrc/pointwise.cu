@@ -68,62 +68,73 @@ PG_DEV void pw_elem(uint64_t& x, uint64_t y, uint64_t z, const Barrett& m, uint6
     if constexpr (OP == PW_SHOUP_PREPARE) x = shoup_quotient(y, m);
 }
 
+// grid: y over polys, x over the L*N/2 element pairs of one poly (32-bit index)
 template <int OP>
 __global__ void __launch_bounds__(256) pw_kernel(PwArgs a) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.pairs; i += stride) {
-        const uint64_t e = 2 * i;  // first element index
-        const uint32_t limb = (uint32_t)((e >> a.log_n) % a.L);
-        const Barrett m = a.bar[limb];
-        const uint64_t ri = a.rhs_pairs ? i % a.rhs_pairs : i;
-        ulonglong2 x = reinterpret_cast<ulonglong2*>(a.x)[i];
-        ulonglong2 y = make_ulonglong2(0, 0), z = make_ulonglong2(0, 0);
-        if constexpr (OP != PW_NEG && OP != PW_MUL_SCALAR) y = __ldg(reinterpret_cast<const ulonglong2*>(a.y) + ri);
-        if constexpr (OP == PW_ADD_MUL || OP == PW_MUL_PREPARED)
-            z = __ldg(reinterpret_cast<const ulonglong2*>(a.z) + ri);
-        const uint64_t sc = (OP == PW_MUL_SCALAR || OP == PW_ADD_MUL_SCALAR) ? a.scalars[limb] : 0;
-        uint64_t x0 = x.x, x1 = x.y;
-        pw_elem<OP>(x0, y.x, z.x, m, sc);
-        pw_elem<OP>(x1, y.y, z.y, m, sc);
-        reinterpret_cast<ulonglong2*>(a.x)[i] = make_ulonglong2(x0, x1);
+    const uint32_t pp = (uint32_t)((a.L << a.log_n) >> 1);  // pairs per poly
+    const uint64_t polys = a.pairs / pp;
+    for (uint64_t p = blockIdx.y; p < polys; p += gridDim.y) {
+        ulonglong2* xp = reinterpret_cast<ulonglong2*>(a.x) + p * pp;
+        const uint64_t roff = a.rhs_pairs ? 0 : p * pp;
+        for (uint32_t ix = blockIdx.x * blockDim.x + threadIdx.x; ix < pp; ix += gridDim.x * blockDim.x) {
+            const uint32_t limb = (2 * ix) >> a.log_n;
+            const Barrett m = a.bar[limb];
+            const uint64_t ri = roff + ix;
+            ulonglong2 x = xp[ix];
+            ulonglong2 y = make_ulonglong2(0, 0), z = make_ulonglong2(0, 0);
+            if constexpr (OP != PW_NEG && OP != PW_MUL_SCALAR)
+                y = __ldg(reinterpret_cast<const ulonglong2*>(a.y) + ri);
+            if constexpr (OP == PW_ADD_MUL || OP == PW_MUL_PREPARED)
+                z = __ldg(reinterpret_cast<const ulonglong2*>(a.z) + ri);
+            const uint64_t sc = (OP == PW_MUL_SCALAR || OP == PW_ADD_MUL_SCALAR) ? a.scalars[limb] : 0;
+            uint64_t x0 = x.x, x1 = x.y;
+            pw_elem<OP>(x0, y.x, z.x, m, sc);
+            pw_elem<OP>(x1, y.y, z.y, m, sc);
+            xp[ix] = make_ulonglong2(x0, x1);
+        }
     }
 }
 
 // butterfly_mul_factor_inplace (primus_poly/src/dcrt/mul.rs:119-155):
-// a' = a + s, b = (a - s) * w with w Shoup-prepared (values w, quotients wq)
+// a' = a + s, b = (a - s) * w with w Shoup-prepared (values w, quotients wq);
+// grid: y over polys, x over the L*N elements of one poly
 __global__ void __launch_bounds__(256) butterfly_kernel(uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
                                                         const uint64_t* __restrict__ w, const uint64_t* __restrict__ wq,
                                                         uint64_t* __restrict__ b, const uint64_t* __restrict__ moduli,
-                                                        uint64_t total, uint64_t period, uint32_t log_n, uint32_t L) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
-        const uint32_t limb = (uint32_t)((i >> log_n) % L);
-        const uint64_t q = moduli[limb];
-        const uint64_t wi = i % period;
-        const uint64_t av = a[i], sv = s[i];
-        a[i] = add_mod(av, sv, q);
-        b[i] = shoup_mul(__ldg(w + wi), __ldg(wq + wi), sub_mod(av, sv, q), q);
+                                                        uint64_t polys, uint32_t log_n, uint32_t L) {
+    const uint32_t ln = L << log_n;
+    for (uint64_t p = blockIdx.y; p < polys; p += gridDim.y) {
+        const uint64_t off = p * ln;
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < ln; lx += gridDim.x * blockDim.x) {
+            const uint64_t q = moduli[lx >> log_n];
+            const uint64_t av = a[off + lx], sv = s[off + lx];
+            a[off + lx] = add_mod(av, sv, q);
+            b[off + lx] = shoup_mul(__ldg(w + lx), __ldg(wq + lx), sub_mod(av, sv, q), q);
+        }
     }
 }
 
 // seeded uniform fill: row r (= poly*L + limb) uses stream stream0 + r
 __global__ void __launch_bounds__(256) fill_uniform_kernel(uint64_t* out, const uint64_t* __restrict__ moduli,
-                                                           uint64_t total, uint32_t log_n, uint32_t L, uint64_t seed,
+                                                           uint64_t polys, uint32_t log_n, uint32_t L, uint64_t seed,
                                                            uint64_t stream0) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t mask = (1ull << log_n) - 1;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
-        const uint64_t row = i >> log_n;
-        out[i] = uniform_at(seed, stream0 + row, i & mask, moduli[row % L]);
+    const uint32_t ln = L << log_n;
+    const uint32_t mask = (1u << log_n) - 1;
+    for (uint64_t p = blockIdx.y; p < polys; p += gridDim.y) {
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < ln; lx += gridDim.x * blockDim.x) {
+            const uint32_t limb = lx >> log_n;
+            out[p * ln + lx] = uniform_at(seed, stream0 + p * L + limb, lx & mask, moduli[limb]);
+        }
     }
 }
 
-static unsigned grid_for(uint64_t work) {
-    // up to 16 resident 256-thread CTAs on each of the 148 SMs
-    const uint64_t cap = 148ull * 16;
-    uint64_t b = (work + 255) / 256;
-    return (unsigned)std::max<uint64_t>(1, std::min(b, cap));
+// x over the elements of one poly (256 threads per CTA), y over polys
+static dim3 grid2(uint64_t inner, uint64_t polys) {
+    const uint64_t bx = std::min<uint64_t>((inner + 255) / 256, 4096);
+    const uint64_t by = std::min<uint64_t>(polys, 65535);
+    return dim3((unsigned)std::max<uint64_t>(bx, 1), (unsigned)std::max<uint64_t>(by, 1));
 }
+
 
 template <int OP>
 static int launch_pw(const pg_ntt_table* t, uint64_t* x, const uint64_t* y, const uint64_t* z,
@@ -154,7 +165,7 @@ static int launch_pw(const pg_ntt_table* t, uint64_t* x, const uint64_t* y, cons
         PG_CUDA(cudaMemcpyAsync(d_sc, h_scalars, t->L * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         a.scalars = d_sc;
     }
-    pw_kernel<OP><<<grid_for(a.pairs), 256, 0, st>>>(a);
+    pw_kernel<OP><<<grid2((uint64_t)t->L * t->n / 2, polys), 256, 0, st>>>(a);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (d_sc) scratch_free(d_sc, st);
@@ -220,8 +231,9 @@ int pg_dcrt_butterfly_mul_factor(const pg_ntt_table* t, uint64_t* d_a, const uin
     if (polys == 0) return PG_OK;
     if (!d_a || !d_s || !d_w || !d_wq || !d_b) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL operand");
     const uint64_t total = (uint64_t)polys * t->L * t->n;
-    butterfly_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(d_a, d_s, d_w, d_wq, d_b, t->d_moduli, total,
-                                                                         (uint64_t)t->L * t->n, t->log_n, t->L);
+    (void)total;
+    butterfly_kernel<<<grid2((uint64_t)t->L * t->n, polys), 256, 0, (cudaStream_t)stream>>>(
+        d_a, d_s, d_w, d_wq, d_b, t->d_moduli, polys, t->log_n, t->L);
     count_launch();
     PG_LAUNCH_CHECK("butterfly_kernel launch");
     return PG_OK;
@@ -233,8 +245,9 @@ int pg_fill_uniform(const pg_ntt_table* t, uint64_t* d_out, size_t polys, uint64
     if (polys == 0) return PG_OK;
     if (!d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "output is NULL");
     const uint64_t total = (uint64_t)polys * t->L * t->n;
-    fill_uniform_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(d_out, t->d_moduli, total, t->log_n, t->L,
-                                                                            seed, stream0);
+    (void)total;
+    fill_uniform_kernel<<<grid2((uint64_t)t->L * t->n, polys), 256, 0, (cudaStream_t)stream>>>(
+        d_out, t->d_moduli, polys, t->log_n, t->L, seed, stream0);
     count_launch();
     PG_LAUNCH_CHECK("fill_uniform_kernel launch");
     return PG_OK;
