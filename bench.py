@@ -233,6 +233,12 @@ def run_gpu(args):
     tab.forward(plain, 1, stream=stream)
     tab.shoup_prepare(plain, plain_q, 1, stream=stream)
     stream.synchronize()
+    # kernel shape per (N, L): the autotuner times every shape of N = 2^16 on this
+    # table before the warm-up and keeps the fastest in the table
+    tuning = tab.autotune(POLYS)
+    rt_shape = tuning["round_trip"]
+    kernel_name = ("ntt_cluster_kernel<16,12,4,RT,fast>" if rt_shape["variant"] == 0
+                   else "ntt_cluster_kernel<16,13,4,RT,fast>")
 
     def step():
         tab.polymul_ntt_plain(data, plain, plain_q, POLYS, stream=stream)
@@ -315,19 +321,23 @@ def run_gpu(args):
             workloads = {"polymul_n1024": bench_polymul_1024(P, stream),
                          "uneven_batch": bench_uneven(P, stream),
                          "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu),
-                         "served_mixed": bench_served(P, stream)}
+                         "served_mixed": bench_served(P, stream),
+                         "autotune_L24": bench_autotune(P)}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues, device generator)",
-            "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+            "config": dict(WORKLOAD, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                           kernel_shape=f"{rt_shape['name']} (autotuned: "
+                                        + ", ".join(f"{k} {tuning[k]['name']} {tuning[k]['us']:.0f} us"
+                                                    for k in ('forward', 'inverse', 'round_trip')) + ")"),
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "ms_per_step": e2e_ms, "path": "pg_memcpy_h2d -> pg_dcrt_polymul_ntt_plain -> pg_memcpy_d2h"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,
-                         "kernel": "ntt_cluster_kernel<16,12,4,RT,fast> (fused fwd -> x plain -> inv)",
+                         "kernel": kernel_name + " (fused fwd -> x plain -> inv)",
                          "algorithmic_bytes_per_launch": ALGO_BYTES},
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
@@ -458,6 +468,22 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
     return res
 
 
+def bench_autotune(P):
+    """Kernel shape chosen by the autotuner for each ring degree (L = 24 primes,
+    about 2^24 residues per launch), with the default shape's time beside it."""
+    out = {}
+    for ln in range(10, 17):
+        n = 1 << ln
+        t = P.DcrtTable(ln, P.ntt_primes(1 << 50, 2 * n, 24))
+        polys = max(1, (1 << 24) // (n * 24))
+        r = t.autotune(polys)
+        out[f"N=2^{ln}"] = {k: {"shape": r[k]["name"], "us": round(r[k]["us"], 1),
+                                "default_us": round(r[k]["default_us"], 1)}
+                            for k in ("forward", "inverse", "round_trip")}
+        out[f"N=2^{ln}"]["polys"] = polys
+    return out
+
+
 def bench_served(P, stream, count=2000, seed=0x5EED0005):
     """Mixed request stream: 50% RNS polymul (N = 2^12..2^16, L = 4..24), 30%
     external product (the N = 2048 shape above), 20% hybrid RNS key switch
@@ -467,6 +493,8 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     rng = np.random.default_rng(seed)
     pm_lns = list(range(12, 17))
     pm_tables = {ln: P.DcrtTable(ln, P.ntt_primes(1 << 50, 2 << ln, 24)) for ln in pm_lns}
+    for t in pm_tables.values():  # kernel shapes per degree, as a serving process would at start-up
+        t.autotune(max(1, (1 << 22) // (t.n * 24)))
     pm_batch = P.PolymulBatch(list(pm_tables.values()))
     xq = P.prev_prime_congruent(1 << 54, 4096)
     xt = P.DcrtTable(11, [xq])
@@ -476,6 +504,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     # hybrid key switch: Q = 16 primes, P = 4 special primes, 4-limb digit groups
     ks_moduli = P.ntt_primes(1 << 50, 1 << 16, 20)
     kt = P.DcrtTable(15, ks_moduli)
+    kt.autotune(8)
     kq = P.DcrtTable(15, ks_moduli[:16])  # Q limbs only, for the input generator
     hks = P.HybridKeySwitch(kt, 16, 4, 4)
     kkey = P.DeviceBuffer(hks.dnum * 2 * 20 * 32768)

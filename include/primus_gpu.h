@@ -105,6 +105,26 @@ typedef struct pg_ntt_table pg_ntt_table;
 int pg_ntt_table_create(uint32_t log_n, const uint64_t *h_moduli, uint32_t moduli_count,
                         pg_ntt_table **out);
 int pg_ntt_table_destroy(pg_ntt_table *table);
+/* NTT kernel shapes.  Each ring degree has a default shape (rows per CTA,
+ * elements per thread, cluster size) and, for N = 2^10 .. 2^16, alternatives
+ * that compute identical values at different speed.  pg_ntt_autotune times
+ * every shape of the table's degree on `polys` seeded polys of its moduli (at
+ * most 1 GiB) for the canonical forward, the inverse and the fused round trip,
+ * and keeps the fastest of each in the table; the lazy forward always runs the
+ * default shape.  It allocates its own buffers and synchronizes; call it before
+ * the table is shared between threads or streams.  No reference counterpart
+ * (the reference's CPU transforms have one shape). */
+typedef struct pg_ntt_tuning {
+    int32_t variant[3]; /* chosen shape per mode: forward, inverse, round trip */
+    float us[3];        /* its time per launch over `rows` rows */
+    float default_us[3];/* the default shape's time, for comparison */
+    uint64_t rows;
+} pg_ntt_tuning;
+enum { PG_NTT_MODE_FORWARD = 0, PG_NTT_MODE_INVERSE = 1, PG_NTT_MODE_ROUND_TRIP = 2 };
+int pg_ntt_autotune(pg_ntt_table *table, size_t polys, pg_ntt_tuning *out);
+int pg_ntt_variant_count(uint32_t log_n);
+const char *pg_ntt_variant_name(uint32_t log_n, int variant); /* NULL if out of range */
+int pg_ntt_set_variant(pg_ntt_table *table, int mode, int variant);
 /* poly_length(), moduli_count(), crt_poly_length() */
 int pg_ntt_table_info(const pg_ntt_table *table, uint32_t *log_n, uint32_t *moduli_count,
                       size_t *poly_length, size_t *crt_poly_length);

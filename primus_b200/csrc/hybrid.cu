@@ -217,6 +217,7 @@ void make_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_tab
     v.d_inv_n = t->d_inv_n + first;
     v.d_inv_last = t->d_inv_last + first;
     v.d_barrett = t->d_barrett + first;
+    for (int m = 0; m < 3; ++m) v.variant[m] = t->variant[m];
 }
 
 template <typename T>

@@ -79,6 +79,7 @@ struct pg_ntt_table {
     ulonglong2* d_inv_n = nullptr;     // [L] N^-1
     ulonglong2* d_inv_last = nullptr;  // [L] inv_root_powers[N-1] * N^-1
     pg::Barrett* d_barrett = nullptr;  // [L]
+    int variant[3] = {0, 0, 0};        // NTT kernel shape per mode (forward, inverse, round trip)
 };
 
 namespace pg {
@@ -108,6 +109,7 @@ struct NttArgs {
     uint64_t max_modulus;
     uint32_t L;
     int lazy;
+    int variant[3];  // kernel shape per mode (0 = default), chosen by the autotuner
 };
 
 enum NttMode { MODE_FWD = 0, MODE_INV = 1, MODE_RT = 2 };
@@ -151,10 +153,16 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     for (uint64_t m : t->moduli) a.max_modulus = m > a.max_modulus ? m : a.max_modulus;
     a.L = t->L;
     a.lazy = lazy;
+    for (int m = 0; m < 3; ++m) a.variant[m] = t->variant[m];
     return a;
 }
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
+// alternative kernel shapes (ntt_variants.cu): variant 1 .. ntt_variant_count(log_n) - 1
+// of the canonical forward, the inverse and the round trip; identical results
+int ntt_variant_count(uint32_t log_n);
+const char* ntt_variant_name(uint32_t log_n, int variant);
+int launch_ntt_variant(const NttArgs& a, uint32_t log_n, int mode, int variant, cudaStream_t stream);
 
 // hybrid key switch context accessors (Q limb count, ring degree)
 uint32_t hybrid_q_limbs(const pg_hybrid_ks* ks);

@@ -1,0 +1,594 @@
+// Shared NTT kernel templates (forward / inverse / fused round trip) and their
+// launchers, included by ntt.cu (default dispatch) and ntt_variants.cu (the
+// alternative shapes the autotuner times).
+//
+// Negacyclic NTT / INTT kernels for sm_100a.
+//
+// Semantics: the reference's UintNttTable (primus_ntt/src/ntt/primitive.rs).
+//   forward  (lazy_transform_slice :211-232): for gap = N/2 .. 1, chunk c of
+//            size 2*gap uses root_powers[2^s + c] (s = stage); Harvey
+//            butterfly u = x mod 2q; v = w*y (Shoup lazy); x = u+v; y = u+2q-v.
+//   inverse  (lazy_inverse_transform_slice :246-286): for gap = 1 .. N/4,
+//            GS butterfly with inv_root_powers read sequentially; the last
+//            stage (gap N/2) is fused with the N^-1 scaling.
+// Every butterfly is evaluated with the reference's formula on the same
+// operands and stages run in the reference's order, so lazy outputs match the
+// CPU values bit for bit.  Only the assignment of butterflies to threads
+// differs.
+//
+// Layout and schedule (B200):
+//   * N <= 2^13: one CTA owns one row (or several small rows) in shared memory.
+//     Each thread holds E = 2^LOG_E elements in registers and runs LOG_E stages
+//     per round; rounds exchange through padded shared memory (index i is
+//     stored at i + i/16, which keeps 64-bit accesses within two-way bank
+//     conflicts for every round).
+//   * N = 2^14 .. 2^16: a thread-block cluster of C = N / M CTAs owns one row
+//     (512 KiB at N = 2^16) in distributed shared memory, each CTA a block of
+//     M = 2^LOG_M elements (4096 by default).  Forward: each thread takes one
+//     column {gt + j N/E} (coalesced HBM reads), runs the first LOG_E stages in
+//     registers and scatters the results to the CTAs owning the blocks
+//     (st.shared::cluster); the remaining stages run as local rounds.  Inverse
+//     mirrors this.  A row is read from and written to HBM exactly once, also
+//     for the fused fwd -> x plain -> inv round trip.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "internal.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace pg {
+
+PG_DEV int padi(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded(int m) { return m + (m >> 4); }
+
+template <int V>
+struct IC {
+    static constexpr int value = V;
+};
+
+// compile-time loop: f(IC<B>), f(IC<B+1>), ..., f(IC<E_-1>); every index is a
+// constant, so register arrays indexed by it stay in registers
+template <int B, int E_, typename F>
+PG_DEV void static_for(F&& f) {
+    if constexpr (B < E_) {
+        f(IC<B>{});
+        static_for<B + 1, E_>(f);
+    }
+}
+
+// Harvey forward butterfly; x, y in [0, 4q) -> [0, 4q).  nq = 2^64 - q.
+PG_DEV void fwd_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
+    uint64_t u = x >= q2 ? x - q2 : x;
+    uint64_t v = shoup_lazy_nq(w.x, w.y, y, nq);
+    x = u + v;
+    y = u + q2 - v;
+}
+
+// Forward butterfly without the u = x mod 2q step.  Used only where the
+// canonical result is returned (transform_slice, the fused round trip): the
+// bound grows by 2q per stage, so after log2(N) <= 16 stages from [0, 4q) the
+// values stay below 36q < 2^64 for q < 2^58, and the final canonical
+// reduction yields the same residues as the Harvey schedule.
+PG_DEV void fwd_bfly_fast(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
+    uint64_t u = x;
+    uint64_t v = shoup_lazy_nq(w.x, w.y, y, nq);
+    x = u + v;
+    y = u + q2 - v;
+}
+
+// Gentleman-Sande inverse butterfly; x, y in [0, 2q) -> [0, 2q)
+PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
+    uint64_t u = x, v = y;
+    uint64_t s = u + v;
+    x = s >= q2 ? s - q2 : s;
+    y = shoup_lazy_nq(w.x, w.y, u + q2 - v, nq);
+}
+
+// Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+2q-v), canonical
+PG_DEV void inv_last_bfly(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, uint64_t q,
+                          uint64_t nq) {
+    uint64_t u = x, v = y;
+    uint64_t a = shoup_lazy_nq(s.x, s.y, u + v, nq);
+    uint64_t b = shoup_lazy_nq(sr.x, sr.y, u + 2 * q - v, nq);
+    x = a >= q ? a - q : a;
+    y = b >= q ? b - q : b;
+}
+
+// any 64-bit v -> v mod q, using floor(2^64/q) (the high word of the Barrett ratio)
+PG_DEV uint64_t reduce_full(uint64_t v, uint64_t q, uint64_t inv64, uint64_t nq) {
+    uint64_t r = v + nq * mulhi64(inv64, v);
+    return r >= q ? r - q : r;
+}
+
+PG_DEV uint64_t canon4(uint64_t v, uint64_t q, uint64_t q2) {
+    v = v >= q2 ? v - q2 : v;
+    return v >= q ? v - q : v;
+}
+
+// insert LOG_E zero bits at bit position g into t
+template <int LOG_E>
+PG_DEV uint32_t group_base(uint32_t t, int g) {
+    uint32_t lo = t & ((1u << g) - 1u);
+    return ((t >> g) << (g + LOG_E)) | lo;
+}
+
+// two consecutive twiddles (value, quotient, value, quotient) with one 256-bit
+// load; p must be 32-byte aligned (callers guarantee an even index)
+PG_DEV void ldg_tw2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
+    uint64_t a0, a1, b0, b1;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a0), "=l"(a1), "=l"(b0), "=l"(b1) : "l"(p));
+    a = make_ulonglong2(a0, a1);
+    b = make_ulonglong2(b0, b1);
+}
+
+// One forward round over register group x (x[jj] is local index base + (jj << G)
+// of a 2^LOG_M block).  Stage bits P_HI down to P_LO; stage bit p is block stage
+// sp = LOG_M-1-p and uses tw[(tw_base << sp) + (i >> (p+1))], tw_base = C + rank
+// for a cluster block (1 for a whole row).  When a stage needs two or more
+// twiddles their first index is even, so they are fetched in 32-byte pairs.
+template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, bool FAST>
+PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
+                      uint64_t q2, uint64_t nq) {
+    constexpr int E = 1 << LOG_E;
+    static_for<0, P_HI - P_LO + 1>([&](auto it) {
+        constexpr int p = P_HI - decltype(it)::value;
+        constexpr int r = p - G;
+        constexpr int half = 1 << r;
+        constexpr int sp = LOG_M - 1 - p;
+        constexpr int nk = E >> (r + 1);
+        const ulonglong2* row = tw + (tw_base << sp) + (base >> (p + 1));
+        auto bfly_k = [&](auto kk, const ulonglong2 w) {
+            constexpr int k = decltype(kk)::value;
+            static_for<0, half>([&](auto ll) {
+                constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
+                if constexpr (FAST)
+                    fwd_bfly_fast(x[jj], x[jj + half], w, q2, nq);
+                else
+                    fwd_bfly(x[jj], x[jj + half], w, q2, nq);
+            });
+        };
+        if constexpr (nk == 1) {
+            bfly_k(IC<0>{}, __ldg(row));
+        } else {
+            static_for<0, nk / 2>([&](auto kp) {
+                constexpr int k = 2 * decltype(kp)::value;
+                ulonglong2 w0, w1;
+                ldg_tw2(row + k, w0, w1);
+                bfly_k(IC<k>{}, w0);
+                bfly_k(IC<k + 1>{}, w1);
+            });
+        }
+    });
+}
+
+// One inverse round, stage bits P_LO up to P_HI (gap 2^p).  The element at
+// local index i of CTA rank `rank` has row index rank*M + i; stage p uses the
+// inverse powers at N - (N >> p) + ((rank*M + i) >> (p+1)) of the device table,
+// which stores inv_root_powers[j + 1] at j (so paired loads are aligned).  The
+// last stage of the transform (p == LOG_N-1) is the N^-1-scaled one.
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI>
+PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
+                      const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq) {
+    const uint64_t q2 = 2 * q;
+    constexpr int E = 1 << LOG_E;
+    constexpr uint32_t N = 1u << LOG_N;
+    static_for<0, P_HI - P_LO + 1>([&](auto it) {
+        constexpr int p = P_LO + decltype(it)::value;
+        constexpr int r = p - G;
+        constexpr int half = 1 << r;
+        constexpr int nk = E >> (r + 1);
+        if constexpr (p == LOG_N - 1) {
+            const ulonglong2 s = *sptr, sr = *srptr;
+            static_for<0, E>([&](auto jt) {
+                constexpr int jj = decltype(jt)::value;
+                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq);
+            });
+        } else {
+            const ulonglong2* row = itw + (N - (N >> p)) + (((rank << LOG_M) + base) >> (p + 1));
+            auto bfly_k = [&](auto kk, const ulonglong2 w) {
+                constexpr int k = decltype(kk)::value;
+                static_for<0, half>([&](auto ll) {
+                    constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
+                    inv_bfly(x[jj], x[jj + half], w, q2, nq);
+                });
+            };
+            if constexpr (nk == 1) {
+                bfly_k(IC<0>{}, __ldg(row));
+            } else {
+                static_for<0, nk / 2>([&](auto kp) {
+                    constexpr int k = 2 * decltype(kp)::value;
+                    ulonglong2 w0, w1;
+                    ldg_tw2(row + k, w0, w1);
+                    bfly_k(IC<k>{}, w0);
+                    bfly_k(IC<k + 1>{}, w1);
+                });
+            }
+        }
+    });
+}
+
+template <int LOG_E, int G>
+PG_DEV void load_smem(uint64_t (&x)[1 << LOG_E], const uint64_t* sm, uint32_t base) {
+    // base and jj << G have disjoint bits, so padi(base | off) = padi(base) + padi(off)
+    const uint64_t* p = sm + padi(base);
+#pragma unroll
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) x[jj] = p[padi(jj << G)];
+}
+
+template <int LOG_E, int G>
+PG_DEV void store_smem(const uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t base) {
+    uint64_t* p = sm + padi(base);
+#pragma unroll
+    for (int jj = 0; jj < (1 << LOG_E); ++jj) p[padi(jj << G)] = x[jj];
+}
+
+// Forward rounds over the low TOP bits of a block (the bits above TOP were
+// processed earlier): round R covers bits [P_LO, P_HI], its group spans
+// [P_LO, P_LO + LOG_E).
+template <int TOP, int LOG_E, int R>
+struct FwdRounds {
+    static constexpr int P_HI = TOP - 1 - R * LOG_E;
+    static constexpr int P_LO = (P_HI - LOG_E + 1) > 0 ? (P_HI - LOG_E + 1) : 0;
+    static constexpr int G = P_LO;
+    static constexpr bool LAST = (P_LO == 0);
+    static constexpr int COUNT = (TOP + LOG_E - 1) / LOG_E;
+};
+
+// Runs forward rounds R..last; x holds round R-1's group on entry (stored to
+// smem first).  On exit x holds the last round's group (G = 0: E contiguous
+// elements at tid*E).
+template <int LOG_M, int TOP, int LOG_E, int R, bool FAST>
+PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
+                     const ulonglong2* __restrict__ tw, uint64_t q2, uint64_t nq) {
+    if constexpr (R < FwdRounds<TOP, LOG_E, 0>::COUNT) {
+        using Cur = FwdRounds<TOP, LOG_E, R>;
+        using Prev = FwdRounds<TOP, LOG_E, R - 1>;
+        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+        __syncthreads();
+        const uint32_t base = group_base<LOG_E>(tid, Cur::G);
+        load_smem<LOG_E, Cur::G>(x, sm, base);
+        fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO, FAST>(x, base, tw_base, tw, q2, nq);
+        fwd_rest<LOG_M, TOP, LOG_E, R + 1, FAST>(x, sm, tid, tw_base, tw, q2, nq);
+    }
+}
+
+template <int TOP, int LOG_E, int R>
+struct InvRounds {
+    static constexpr int P_LO = R * LOG_E;
+    static constexpr int P_HI = (P_LO + LOG_E - 1) < (TOP - 1) ? (P_LO + LOG_E - 1) : (TOP - 1);
+    static constexpr int G = P_LO < (TOP - LOG_E) ? P_LO : (TOP - LOG_E);
+    static constexpr bool LAST = (P_HI == TOP - 1);
+    static constexpr int COUNT = (TOP + LOG_E - 1) / LOG_E;
+};
+
+// Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
+// (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
+template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END>
+PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
+                      const ulonglong2* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
+                      uint64_t nq) {
+    if constexpr (R < R_END) {
+        using Cur = InvRounds<TOP, LOG_E, R>;
+        using Prev = InvRounds<TOP, LOG_E, R - 1>;
+        store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+        __syncthreads();
+        const uint32_t base = group_base<LOG_E>(tid, Cur::G);
+        load_smem<LOG_E, Cur::G>(x, sm, base);
+        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, sptr, srptr, q, nq);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, sptr, srptr, q, nq);
+    }
+}
+
+// ============================================================================
+// Single-CTA kernel: ROWS rows of N = 2^LOG_N per CTA, T = N/E threads per row.
+// FAST selects the forward schedule without per-butterfly reduction of u (only
+// when the caller needs canonical or multiplied outputs and every q < 2^58).
+// ============================================================================
+template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
+__global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kernel(NttArgs a) {
+    constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E;
+    extern __shared__ uint64_t smem_block[];
+    const uint32_t tid = threadIdx.x;
+    // launch order is limb-major (all polys of limb 0, then limb 1, ...) so that
+    // concurrently running CTAs share one prime's twiddles in L2
+    const uint64_t u = (uint64_t)blockIdx.x * ROWS + threadIdx.y;
+    const bool active = u < a.rows;
+    const uint64_t polys = a.desc ? 1 : a.rows / a.L;  // descriptor rows need no [P][L] shape
+    uint32_t limb = active ? (uint32_t)(u / polys) : 0;
+    const uint64_t row = active ? (u % polys) * a.L + limb : 0;
+    uint64_t* sm = smem_block + threadIdx.y * padded(N);
+    uint64_t* g = a.data + row * N;
+    const uint64_t* mulp = nullptr;
+    if (a.desc) {  // descriptor-driven rows (ragged batches)
+        const RowDesc d = a.desc[active ? u : 0];
+        g = d.data;
+        limb = d.limb;
+        mulp = d.mul;
+    }
+    const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
+    uint64_t x[E];
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        using R0 = FwdRounds<LOG_N, LOG_E, 0>;
+        // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = active ? g[tid + jj * T] : 0;
+        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, tw, q2, nq);
+        fwd_rest<LOG_N, LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, tw, q2, nq);
+        // x = E contiguous outputs at tid*E
+        if constexpr (MODE == MODE_FWD) {
+            if constexpr (FAST) {
+                const uint64_t inv64 = a.bar[limb].r1;
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+            } else if (!a.lazy) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
+            }
+            __syncthreads();
+            store_smem<LOG_E, 0>(x, sm, tid * E);
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < E; ++k) g[tid + k * T] = sm[padi(tid + k * T)];
+            }
+        } else {
+            // pointwise product with the NTT-domain plaintext (Shoup-prepared);
+            // the lazy product in [0, 2q) is a valid inverse input
+            const uint64_t* pv = a.plain + (size_t)limb * N + tid * E;
+            const uint64_t* pq = a.plain_q + (size_t)limb * N + tid * E;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+        }
+    }
+    // ---------------- inverse
+    if constexpr (MODE != MODE_FWD) {
+        const ulonglong2* itw = a.inv + (size_t)limb * N;
+        const ulonglong2* sptr = a.inv_n + limb;
+        const ulonglong2* srptr = a.inv_last + limb;
+        using I0 = InvRounds<LOG_N, LOG_E, 0>;
+        if constexpr (MODE == MODE_INV) {
+            // stage the bit-reversed row through smem (coalesced), then round 0
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                uint64_t v = active ? g[tid + k * T] : 0;
+                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+                if (mulp && active) v = barrett_mul(v, mulp[tid + k * T], a.bar[limb]);
+                sm[padi(tid + k * T)] = v;
+            }
+            __syncthreads();
+            load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
+        } else {
+            // round trip: the forward's last group (tid*E .. tid*E+E-1) is the
+            // inverse's first group (I0::G == 0), so it stays in registers
+            static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
+        }
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr, srptr,
+                                                                  q, nq);
+        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT>(x, sm, tid, 0, itw, sptr, srptr, q, nq);
+        // last group: elements tid + jj*T, coalesced store
+        using Last = InvRounds<LOG_N, LOG_E, I0::COUNT - 1>;
+        static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
+        if (active) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) g[tid + jj * T] = x[jj];
+        }
+    }
+}
+
+// ============================================================================
+// Cluster kernel: a row of N = 2^LOG_N is owned by C = 2^(LOG_N - LOG_M) CTAs.
+//   cross phase: thread gt = rank*T + tid owns the column {gt + jj*N/E} (the
+//     top LOG_E index bits vary), i.e. the first LOG_E forward stages (last
+//     LOG_E inverse stages); coalesced HBM access.
+//   local phase: CTA rank owns block [rank*M, (rank+1)*M) in shared memory and
+//     runs the remaining stages in rounds of LOG_E.
+// The two phases exchange through distributed shared memory
+// (st.shared::cluster) between cluster barriers.
+// ============================================================================
+PG_DEV void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
+PG_DEV void cluster_arrive_release() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+PG_DEV void cluster_wait_acquire() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
+PG_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// st.shared::cluster of one u64 into CTA `rank`'s shared memory at the same offset
+PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(remote) : "r"(local_addr), "r"(rank));
+    asm volatile("st.shared::cluster.u64 [%0], %1;\n" ::"r"(remote), "l"(v) : "memory");
+}
+
+// CTAs per SM the register budget is sized for: the whole 64K-entry register
+// file is shared by MINB CTAs of T threads, i.e. 65536 / (MINB * T) registers
+// per thread (64 for the shapes below), so independent CTAs overlap each
+// other's barrier and exchange phases.
+__host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
+
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
+    ntt_cluster_kernel(NttArgs a) {
+    constexpr int LOG_C = LOG_N - LOG_M;
+    constexpr int N = 1 << LOG_N, M = 1 << LOG_M, E = 1 << LOG_E, LOG_T = LOG_M - LOG_E, T = 1 << LOG_T;
+    constexpr int LOG_K = LOG_E - LOG_C;  // top block bits handled by the cross phase
+    constexpr int K = 1 << LOG_K;
+    constexpr int TOP = LOG_M - LOG_K;    // block bits handled by the local rounds
+    constexpr int GX = LOG_N - LOG_E;     // cross group stride bit (N/E)
+    static_assert(LOG_K >= 0 && TOP >= LOG_E, "shape");
+    extern __shared__ uint64_t smem_cl[];
+    uint64_t* sm = smem_cl;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t rank = blockIdx.x & ((1 << LOG_C) - 1);
+    // grid is exactly rows * C; clusters run limb-major so that concurrently
+    // running clusters share one prime's twiddles in L2
+    const uint64_t u = blockIdx.x >> LOG_C;
+    const uint64_t polys = a.desc ? 1 : a.rows / a.L;  // descriptor rows need no [P][L] shape
+    uint32_t limb = (uint32_t)(u / polys);
+    const uint64_t row = (u % polys) * a.L + limb;
+    uint64_t* g = a.data + row * N;
+    const uint64_t* mulp = nullptr;
+    if (a.desc) {  // descriptor-driven rows (ragged batches)
+        const RowDesc d = a.desc[u];
+        g = d.data;
+        limb = d.limb;
+        mulp = d.mul;
+    }
+    const uint64_t q = a.moduli[limb], nq = 0 - q;
+    const uint32_t gt = (rank << LOG_T) + tid;  // cross group (column) of this thread
+    uint64_t x[E];
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+        const uint64_t q2 = q << 1;
+        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        // matched by the wait before the first remote store; relaxed is enough
+        // because this CTA has not touched shared memory yet
+        cluster_arrive_relaxed();
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = g[gt + (jj << GX)];
+        fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, FAST>(x, gt, 1, tw, q2, nq);
+        cluster_wait_acquire();  // every CTA of the cluster is running
+        // element gt + jj*N/E lives in block jj >> LOG_K at local index gt + (jj & (K-1)) * N/E
+        const uint32_t la = smem_u32(sm + padi(gt));
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj)
+            st_cluster(la + 8 * padi((jj & (K - 1)) << GX), (uint32_t)(jj >> LOG_K), x[jj]);
+        cluster_arrive_release();
+        cluster_wait_acquire();
+        // local rounds over the low TOP block bits
+        using R0 = FwdRounds<TOP, LOG_E, 0>;
+        load_smem<LOG_E, R0::G>(x, sm, group_base<LOG_E>(tid, R0::G));
+        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, group_base<LOG_E>(tid, R0::G), (1u << LOG_C) + rank,
+                                                                 tw, q2, nq);
+        fwd_rest<LOG_M, TOP, LOG_E, 1, FAST>(x, sm, tid, (1u << LOG_C) + rank, tw, q2, nq);
+        if constexpr (MODE == MODE_FWD) {
+            if constexpr (FAST) {
+                const uint64_t inv64 = a.bar[limb].r1;
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+            } else if (!a.lazy) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = canon4(x[jj], q, q2);
+            }
+            __syncthreads();
+            store_smem<LOG_E, 0>(x, sm, tid * E);
+            __syncthreads();
+            uint64_t* gb = g + rank * M;
+#pragma unroll
+            for (int k = 0; k < E; ++k) gb[tid + k * T] = sm[padi(tid + k * T)];
+        } else {
+            const uint64_t* pv = a.plain + (size_t)limb * N + rank * M + tid * E;
+            const uint64_t* pq = a.plain_q + (size_t)limb * N + rank * M + tid * E;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+        }
+    }
+    // ---------------- inverse
+    if constexpr (MODE != MODE_FWD) {
+        const ulonglong2* itw = a.inv + (size_t)limb * N;
+        using I0 = InvRounds<TOP, LOG_E, 0>;
+        using ILast = InvRounds<TOP, LOG_E, I0::COUNT - 1>;
+        static_assert(I0::COUNT >= 2, "cluster path needs two local rounds");
+        if constexpr (MODE == MODE_INV) {
+            uint64_t* gb = g + rank * M;
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                uint64_t v = gb[tid + k * T];
+                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+                if (mulp) v = barrett_mul(v, mulp[rank * M + tid + k * T], a.bar[limb]);
+                sm[padi(tid + k * T)] = v;
+            }
+            __syncthreads();
+            load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
+        }
+        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, nullptr,
+                                                                  nullptr, q, nq);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1>(x, sm, tid, rank, itw, nullptr, nullptr, q, nq);
+        {
+            // last local round: its smem loads precede the cluster arrive, so no
+            // CTA overwrites a block that another CTA is still reading
+            using Prev = InvRounds<TOP, LOG_E, I0::COUNT - 2>;
+            store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
+            __syncthreads();
+            const uint32_t base = group_base<LOG_E>(tid, ILast::G);
+            load_smem<LOG_E, ILast::G>(x, sm, base);
+            // release: these shared-memory reads must be performed before any
+            // other CTA, released by this barrier, overwrites the block
+            cluster_arrive_release();
+            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, nullptr, nullptr, q,
+                                                                               nq);
+            cluster_wait_acquire();
+            // element at row index i = rank*M + base + (jj << G) belongs to cross
+            // group c = i mod N/E (CTA c >> LOG_T, thread c mod T) as element i >> GX:
+            // it goes to slot (i >> GX) * T + (c mod T) of that CTA's buffer
+            const uint32_t i0 = (rank << LOG_M) + base;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) {
+                const uint32_t i = i0 + ((uint32_t)jj << ILast::G);
+                const uint32_t c = i & ((1u << GX) - 1);
+                st_cluster(smem_u32(sm + padi(((i >> GX) << LOG_T) + (c & (T - 1)))), c >> LOG_T, x[jj]);
+            }
+            cluster_arrive_release();
+            cluster_wait_acquire();
+        }
+        // cross inverse stages (the last LOG_E, including the N^-1-scaled one)
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = sm[padi((jj << LOG_T) + tid)];
+        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1>(x, gt, 0, itw, a.inv_n + limb, a.inv_last + limb, q, nq);
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
+    }
+}
+
+}  // namespace pg
+
+namespace pg {
+
+template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
+static int launch_block(const NttArgs& a, cudaStream_t st) {
+    constexpr int T = 1 << (LOG_N - LOG_E);
+    constexpr size_t smem = (size_t)ROWS * padded(1 << LOG_N) * sizeof(uint64_t);
+    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE, FAST>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return cuda_status(attr, "ntt_block_kernel: shared memory attribute");
+    dim3 block(T, ROWS);
+    dim3 grid((unsigned)((a.rows + ROWS - 1) / ROWS));
+    kern<<<grid, block, smem, st>>>(a);
+    count_launch();
+    PG_LAUNCH_CHECK("ntt_block_kernel launch");
+    return PG_OK;
+}
+
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
+static int launch_cluster(const NttArgs& a, cudaStream_t st) {
+    constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
+    constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, FAST>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
+    if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.rows * C));
+    cfg.blockDim = dim3(T);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if constexpr (C > 8) {
+        static const cudaError_t np = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (np != cudaSuccess) return cuda_status(np, "ntt_cluster_kernel: non-portable cluster size");
+    }
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    count_launch();
+    if (e != cudaSuccess) return cuda_status(e, "ntt_cluster_kernel launch");
+    return PG_OK;
+}
+
+}  // namespace pg

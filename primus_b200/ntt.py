@@ -59,6 +59,21 @@ def host_tables(log_n: int, q: int) -> dict:
     return d
 
 
+class NttTuning(C.Structure):
+    _fields_ = [("variant", C.c_int32 * 3), ("us", C.c_float * 3), ("default_us", C.c_float * 3),
+                ("rows", C.c_uint64)]
+
+
+def variant_count(log_n: int) -> int:
+    """Kernel shapes available for degree 2^log_n (0 is the default)."""
+    return int(nat.lib().pg_ntt_variant_count(log_n))
+
+
+def variant_name(log_n: int, variant: int) -> str:
+    r = nat.lib().pg_ntt_variant_name(log_n, variant)
+    return r.decode() if r else ""
+
+
 class DcrtTable:
     """Device-resident NTT tables for L primes of degree N = 2^log_n
     (UintCrtNttTable, primus_ntt/src/dcrt/primitive.rs)."""
@@ -167,6 +182,21 @@ class DcrtTable:
 
     def fill_uniform(self, buf: DeviceBuffer, polys: int, seed: int, stream0: int = 0, stream=None):
         call("pg_fill_uniform", self.h, buf.ptr, polys, seed, stream0, _sh(stream))
+
+    # ---- kernel shapes (autotuner)
+    def autotune(self, polys: int) -> dict:
+        """Time every kernel shape of this degree on `polys` seeded polys and keep
+        the fastest per mode in the table (pg_ntt_autotune)."""
+        r = NttTuning()
+        call("pg_ntt_autotune", self.h, polys, C.byref(r))
+        names = ["forward", "inverse", "round_trip"]
+        return {n: {"variant": r.variant[i], "name": variant_name(self.log_n, r.variant[i]), "us": r.us[i],
+                    "default_us": r.default_us[i]}
+                for i, n in enumerate(names)} | {"rows": r.rows}
+
+    def set_variant(self, mode: int, variant: int):
+        """Force kernel shape `variant` for mode 0 (canonical forward), 1 (inverse) or 2 (round trip)."""
+        call("pg_ntt_set_variant", self.h, mode, variant)
 
     # ---- pointwise (device)
     def mul(self, x, y, polys, rhs_polys=None, stream=None):
