@@ -114,7 +114,10 @@ __global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
                         const ulonglong2 w = mat[j * ag + m];
                         y += shoup_lazy(w.x, w.y, tv[m], rq);
                     }
-                dst[(size_t)r * a.N] = reduce_below_16q(y, rq);
+                // [0, 4 r) is enough: the forward NTT that follows accepts inputs below
+                // 4q and returns canonical values of the same residues
+                if (AMAX > 4) y = y >= 8 * rq ? y - 8 * rq : y;
+                dst[(size_t)r * a.N] = y >= 4 * rq ? y - 4 * rq : y;
             }
         }
     }

@@ -62,71 +62,85 @@ struct MacArgs {
     int negate;
 };
 
-// One thread per (batch chunk, output poly c, limb l, coefficient x): each key
-// element is loaded once per chunk of kMacChunk ciphertexts and multiplied into
-// every ciphertext's accumulator of the chunk, so a batch reads the key
-// ceil(B / kMacChunk) times instead of B times.  Grid: x over the L*N
-// coefficients of a poly (32-bit index), y over (chunk, c), so that no thread
-// divides 64-bit indices.
-constexpr uint32_t kMacChunk = 4;
+// One thread per (chunk of kMacChunk ciphertexts, pair of output polys, limb l,
+// coefficient x); lanes run over consecutive coefficients (coalesced).  Each
+// digit element is loaded once for both output polys of the pair and each key
+// element once for the whole chunk, so a batch reads the digits once per pair
+// of output polys and the key ceil(B / kMacChunk) times.  Grid: x over the
+// coefficients of a poly (32-bit index), y over (chunk, output pair).
+constexpr uint32_t kMacChunk = 2;
+constexpr uint32_t kMacOut = 2;
 
 template <bool FOLD>
-__global__ void __launch_bounds__(256, 2) mac_kernel(MacArgs a) {
+__global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
     const uint32_t LN = a.L * (uint32_t)a.N;
-    const size_t outer = ((a.B + kMacChunk - 1) / kMacChunk) * a.KOUT;
+    const uint32_t pairs = (a.KOUT + kMacOut - 1) / kMacOut;
+    const size_t outer = ((a.B + kMacChunk - 1) / kMacChunk) * pairs;
     const size_t kstride = (size_t)a.KOUT * LN;
     const size_t dstride = (size_t)a.KIN * a.d * LN;  // one ciphertext's digits
     const uint32_t nterms = a.KIN * a.d;
     for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
-        const uint32_t c = (uint32_t)(o % a.KOUT);
-        const size_t b0 = (o / a.KOUT) * kMacChunk;
+        const uint32_t c0 = (uint32_t)(o % pairs) * kMacOut;
+        const uint32_t nc = min(kMacOut, a.KOUT - c0);
+        const size_t b0 = (o / pairs) * kMacChunk;
         const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
         for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
             const uint32_t l = lx >> a.log_n;
             const Barrett m = a.bar[l];
-            uint64_t lo[kMacChunk], hi[kMacChunk];
+            uint64_t lo[kMacOut][kMacChunk], hi[kMacOut][kMacChunk];
 #pragma unroll
-            for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[bb] = hi[bb] = 0;
-            const uint64_t* kp = a.key + (size_t)c * LN + lx;
+            for (uint32_t cc = 0; cc < kMacOut; ++cc)
+#pragma unroll
+                for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[cc][bb] = hi[cc][bb] = 0;
+            const uint64_t* kp = a.key + (size_t)c0 * LN + lx;
             const uint64_t* dp = a.dig + b0 * dstride + lx;
-#pragma unroll 2
             for (uint32_t ij = 0; ij < nterms; ++ij) {
                 if (FOLD && ij && (ij & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
 #pragma unroll
-                    for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-                        lo[bb] = barrett_reduce_2limb(lo[bb], hi[bb], m);
-                        hi[bb] = 0;
-                    }
+                    for (uint32_t cc = 0; cc < kMacOut; ++cc)
+#pragma unroll
+                        for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                            lo[cc][bb] = barrett_reduce_2limb(lo[cc][bb], hi[cc][bb], m);
+                            hi[cc][bb] = 0;
+                        }
                 }
-                const uint64_t kv = __ldg(kp + ij * kstride);
-                uint64_t dv[kMacChunk];
+                uint64_t kv[kMacOut], dv[kMacChunk];
+#pragma unroll
+                for (uint32_t cc = 0; cc < kMacOut; ++cc) kv[cc] = cc < nc ? __ldg(kp + ij * kstride + cc * LN) : 0;
 #pragma unroll
                 for (uint32_t bb = 0; bb < kMacChunk; ++bb) dv[bb] = bb < nb ? __ldg(dp + bb * dstride + ij * LN) : 0;
 #pragma unroll
-                for (uint32_t bb = 0; bb < kMacChunk; ++bb) mac128(lo[bb], hi[bb], kv, dv[bb]);
+                for (uint32_t cc = 0; cc < kMacOut; ++cc)
+#pragma unroll
+                    for (uint32_t bb = 0; bb < kMacChunk; ++bb) mac128(lo[cc][bb], hi[cc][bb], kv[cc], dv[bb]);
             }
 #pragma unroll
-            for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-                if (bb >= nb) break;
-                const size_t b = b0 + bb;
-                const size_t bc = b * a.KOUT + c;
-                const uint64_t s = barrett_reduce_2limb(lo[bb], hi[bb], m);
-                uint64_t r;
-                if (a.negate) {
-                    const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
-                    r = sub_mod(base, s, m.q);
-                } else {
-                    const uint64_t base = a.acc ? a.acc[bc * LN + lx] : 0;
-                    r = add_mod(base, s, m.q);
-                }
-                if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
-                    const uint32_t x = lx & ((uint32_t)a.N - 1);
-                    if (l < a.l_split)
-                        a.out[(bc * a.l_split + l) * a.N + x] = r;
-                    else
-                        a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
-                } else {
-                    a.out[bc * LN + lx] = r;
+            for (uint32_t cc = 0; cc < kMacOut; ++cc) {
+                if (cc >= nc) break;
+                const uint32_t c = c0 + cc;
+#pragma unroll
+                for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                    if (bb >= nb) break;
+                    const size_t b = b0 + bb;
+                    const size_t bc = b * a.KOUT + c;
+                    const uint64_t s = barrett_reduce_2limb(lo[cc][bb], hi[cc][bb], m);
+                    uint64_t r;
+                    if (a.negate) {
+                        const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
+                        r = sub_mod(base, s, m.q);
+                    } else {
+                        const uint64_t base = a.acc ? a.acc[bc * LN + lx] : 0;
+                        r = add_mod(base, s, m.q);
+                    }
+                    if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+                        const uint32_t x = lx & ((uint32_t)a.N - 1);
+                        if (l < a.l_split)
+                            a.out[(bc * a.l_split + l) * a.N + x] = r;
+                        else
+                            a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
+                    } else {
+                        a.out[bc * LN + lx] = r;
+                    }
                 }
             }
         }
@@ -235,7 +249,8 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     a.log_n = t->log_n;
     a.negate = negate;
     if ((size_t)t->L * t->n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
-    const dim3 grid = grid2((size_t)t->L * t->n, ((B + kMacChunk - 1) / kMacChunk) * kout);
+    const size_t LN = (size_t)t->L * t->n;
+    const dim3 grid = grid2(LN, ((B + kMacChunk - 1) / kMacChunk) * ((kout + kMacOut - 1) / kMacOut));
     if (kin * d > 8)  // more than 8 products per output: fold the 128-bit sums every 8
         mac_kernel<true><<<grid, 256, 0, st>>>(a);
     else
