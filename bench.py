@@ -321,6 +321,7 @@ def run_gpu(args):
             workloads = {"polymul_n1024": bench_polymul_1024(P, stream),
                          "uneven_batch": bench_uneven(P, stream),
                          "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu),
+                         "hybrid_ks": bench_hybrid_ks(P, stream),
                          "served_mixed": bench_served(P, stream),
                          "autotune_L24": bench_autotune(P)}
         out = {
@@ -466,6 +467,43 @@ def bench_ext_product(P, stream, batch=4096, cpu=False):
         res["cpu_port_ext_products_per_s"] = sample / dt
         res["cpu_port_sample"] = f"{sample} ciphertexts on {cpu_threads()} threads, {dt:.2f} s"
     return res
+
+
+def bench_hybrid_ks(P, stream, batches=(1, 8, 32)):
+    """Hybrid RNS key switch (N = 2^15, L = 16 primes + K = 4 special primes,
+    4-limb digit groups, k = 1): time per key switch at several batch sizes."""
+    moduli = P.ntt_primes(1 << 50, 1 << 16, 20)
+    kt = P.DcrtTable(15, moduli)
+    kt.autotune(8)
+    kq = P.DcrtTable(15, moduli[:16])
+    hks = P.HybridKeySwitch(kt, 16, 4, 4)
+    key = P.DeviceBuffer(hks.dnum * 2 * 20 * 32768)
+    kt.fill_uniform(key, hks.dnum * 2, seed=0x5EED0006, stream=stream)
+    res = {"workload": "hybrid key switch, N=2^15, L=16 + K=4 special primes, alpha=4 (dnum=4), k=1",
+           "rows_transformed_per_key_switch": 4 * 20 + 4 * 2 + 16 * 2 + 16}
+    for B in batches:
+        di, do = P.DeviceBuffer(B * 2 * 16 * 32768), P.DeviceBuffer(B * 2 * 16 * 32768)
+        kq.fill_uniform(di, 2 * B, seed=0x5EED0007, stream=stream)
+        ws = P.DeviceBuffer(hks.workspace_size(1, 1, B) // 8 + 1)
+        ms = _time_stream(P, stream, lambda: hks.key_switch(1, 1, key, di, do, B, workspace=ws, stream=stream), 5)
+        res[f"batch_{B}"] = {"ms_per_batch": ms, "us_per_key_switch": ms * 1e3 / B,
+                             "key_switches_per_s": B / (ms / 1e3)}
+        del di, do, ws
+    return res
+
+
+def run_workload(args):
+    """One secondary workload alone (for profiler captures and focused runs)."""
+    import primus_b200 as P
+    stream = P.Stream()
+    fn = {"polymul_n1024": lambda: bench_polymul_1024(P, stream),
+          "uneven_batch": lambda: bench_uneven(P, stream),
+          "ext_product": lambda: bench_ext_product(P, stream, cpu=not args.no_cpu),
+          "hybrid_ks": lambda: bench_hybrid_ks(P, stream),
+          "served_mixed": lambda: bench_served(P, stream),
+          "autotune_L24": lambda: bench_autotune(P)}[args.workload]
+    print(json.dumps({"workload_name": args.workload, **fn()}))
+    return 0
 
 
 def bench_autotune(P):
@@ -625,8 +663,14 @@ def main(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--polys", type=int, default=POLYS,
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")
+    ap.add_argument("--workload", default=None,
+                    choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "served_mixed",
+                             "autotune_L24"],
+                    help="run only this secondary workload and print its result")
     args = ap.parse_args(argv)
     set_polys(args.polys)
+    if args.workload:
+        return run_workload(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
