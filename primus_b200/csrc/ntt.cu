@@ -160,7 +160,7 @@ namespace pg {
 #define PG_NTT_LOG_M 12
 #endif
 
-template <int MODE, bool FAST>
+template <int MODE, int FAST>
 static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
     switch (log_n) {
         case 1: return launch_block<1, 1, 128, MODE, FAST>(a, st);
@@ -184,8 +184,6 @@ static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
     }
 }
 
-// fast schedule: every modulus below 2^58 so 36q < 2^64 (see fwd_bfly_fast)
-static bool fast_ok(const NttArgs& a) { return a.max_modulus < (1ull << 58); }
 
 
 // the opt-in maximum of dynamic shared memory per CTA on sm_100 (227 KiB)
@@ -253,17 +251,23 @@ int launch_ext_fused(const pg_ntt_table* t, const GadgetWord& gw, const uint64_t
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
     if (a.rows == 0) return PG_OK;
-    // a tuned shape runs the canonical forward / round trip (fast schedule) and the inverse
-    if (mode >= 0 && mode < 3 && a.variant[mode] > 0 && (mode == MODE_INV || (!a.lazy && fast_ok(a))))
+    const bool ffwd = fast_fwd_ok(a), finv = fast_inv_ok(a);
+    // a tuned shape runs the fast schedules: canonical forward, inverse and round trip
+    if (mode >= 0 && mode < 3 && a.variant[mode] > 0 &&
+        (mode == MODE_FWD ? (!a.lazy && ffwd) : finv))
         return launch_ntt_variant(a, log_n, mode, a.variant[mode], st);
     switch (mode) {
         case MODE_FWD:
-            if (!a.lazy && fast_ok(a)) return launch_mode<MODE_FWD, true>(a, log_n, st);
-            return launch_mode<MODE_FWD, false>(a, log_n, st);
-        case MODE_INV: return launch_mode<MODE_INV, false>(a, log_n, st);
+            if (!a.lazy && ffwd) return launch_mode<MODE_FWD, kSchedFastFwd>(a, log_n, st);
+            return launch_mode<MODE_FWD, kSchedExact>(a, log_n, st);
+        case MODE_INV:
+            // the inverse's outputs are canonical on every schedule (lazy included)
+            if (finv) return launch_mode<MODE_INV, kSchedFastBoth>(a, log_n, st);
+            return launch_mode<MODE_INV, kSchedExact>(a, log_n, st);
         case MODE_RT:
-            if (fast_ok(a)) return launch_mode<MODE_RT, true>(a, log_n, st);
-            return launch_mode<MODE_RT, false>(a, log_n, st);
+            if (finv) return launch_mode<MODE_RT, kSchedFastBoth>(a, log_n, st);
+            if (ffwd) return launch_mode<MODE_RT, kSchedFastFwd>(a, log_n, st);
+            return launch_mode<MODE_RT, kSchedExact>(a, log_n, st);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "bad NTT mode");
 }

@@ -86,15 +86,31 @@ PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, 
     y = shoup_lazy_nq(w.x, w.y, u + q2 - v, nq);
 }
 
-// Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+2q-v), canonical
+// Inverse butterfly without the x reduction, for inputs below `bnd` (a power-of-two
+// multiple of 2q known at compile time): x = u + v (< 2 bnd), y = w (u + bnd - v)
+// in [0, 2q).  Used only where the result is canonical (the inverse always is)
+// and every q < 2^50, so that the unreduced sums stay below 2^64 (see inv_round).
+PG_DEV void inv_bfly_fast(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t bnd, uint64_t nq) {
+    uint64_t u = x, v = y;
+    x = u + v;
+    y = shoup_lazy_nq(w.x, w.y, u + bnd - v, nq);
+}
+
+// Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+bnd-v),
+// canonical; inputs below bnd (2q on the exact schedule)
 PG_DEV void inv_last_bfly(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, uint64_t q,
-                          uint64_t nq) {
+                          uint64_t nq, uint64_t bnd) {
     uint64_t u = x, v = y;
     uint64_t a = shoup_lazy_nq(s.x, s.y, u + v, nq);
-    uint64_t b = shoup_lazy_nq(sr.x, sr.y, u + 2 * q - v, nq);
+    uint64_t b = shoup_lazy_nq(sr.x, sr.y, u + bnd - v, nq);
     x = a >= q ? a - q : a;
     y = b >= q ? b - q : b;
 }
+
+// First stage at which the unreduced inverse schedule reduces its values again:
+// every round that starts at or after this stage first reduces its elements to
+// [0, q).  Before it values grow at most 2^12 q (< 2^62 for q < 2^50).
+constexpr int kFastInvReduceStage = 8;
 
 // any 64-bit v -> v mod q, using floor(2^64/q) (the high word of the Barrett ratio)
 PG_DEV uint64_t reduce_full(uint64_t v, uint64_t q, uint64_t inv64, uint64_t nq) {
@@ -168,22 +184,37 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // inverse powers at N - (N >> p) + ((rank*M + i) >> (p+1)) of the device table,
 // which stores inv_root_powers[j + 1] at j (so paired loads are aligned).  The
 // last stage of the transform (p == LOG_N-1) is the N^-1-scaled one.
-template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI>
+//
+// FASTI (every q < 2^50, inputs below 2q): no per-butterfly reduction of x.  A
+// round that starts before kFastInvReduceStage sees inputs below 2^p * 2q at
+// stage p; a round that starts at or after it first reduces its elements to
+// [0, q) (inv64 = floor(2^64/q)), after which stage p sees inputs below
+// 2^(p - P_LO) * 2q.  Outputs are canonical either way, so the values equal the
+// exact Harvey schedule's.
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, bool FASTI = false>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
-                      const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq) {
+                      const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq,
+                      uint64_t inv64 = 0) {
     const uint64_t q2 = 2 * q;
     constexpr int E = 1 << LOG_E;
     constexpr uint32_t N = 1u << LOG_N;
+    constexpr bool RED = FASTI && P_LO >= kFastInvReduceStage;
+    if constexpr (RED) {
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+    }
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
         constexpr int p = P_LO + decltype(it)::value;
         constexpr int r = p - G;
         constexpr int half = 1 << r;
         constexpr int nk = E >> (r + 1);
+        // bound of this stage's inputs
+        const uint64_t bnd = FASTI ? (q2 << (RED ? p - P_LO : p)) : q2;
         if constexpr (p == LOG_N - 1) {
             const ulonglong2 s = *sptr, sr = *srptr;
             static_for<0, E>([&](auto jt) {
                 constexpr int jj = decltype(jt)::value;
-                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq);
+                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq, bnd);
             });
         } else {
             const ulonglong2* row = itw + (N - (N >> p)) + (((rank << LOG_M) + base) >> (p + 1));
@@ -191,7 +222,10 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
                 constexpr int k = decltype(kk)::value;
                 static_for<0, half>([&](auto ll) {
                     constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
-                    inv_bfly(x[jj], x[jj + half], w, q2, nq);
+                    if constexpr (FASTI)
+                        inv_bfly_fast(x[jj], x[jj + half], w, bnd, nq);
+                    else
+                        inv_bfly(x[jj], x[jj + half], w, q2, nq);
                 });
             };
             if constexpr (nk == 1) {
@@ -265,10 +299,10 @@ struct InvRounds {
 
 // Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
 // (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
-template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END>
+template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END, bool FASTI = false>
 PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
                       const ulonglong2* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
-                      uint64_t nq) {
+                      uint64_t nq, uint64_t inv64 = 0) {
     if constexpr (R < R_END) {
         using Cur = InvRounds<TOP, LOG_E, R>;
         using Prev = InvRounds<TOP, LOG_E, R - 1>;
@@ -276,8 +310,9 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
         __syncthreads();
         const uint32_t base = group_base<LOG_E>(tid, Cur::G);
         load_smem<LOG_E, Cur::G>(x, sm, base);
-        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI>(x, base, rank, itw, sptr, srptr, q, nq);
-        inv_range<LOG_N, LOG_M, TOP, LOG_E, R + 1, R_END>(x, sm, tid, rank, itw, sptr, srptr, q, nq);
+        inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI, FASTI>(x, base, rank, itw, sptr, srptr, q, nq,
+                                                                           inv64);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, R + 1, R_END, FASTI>(x, sm, tid, rank, itw, sptr, srptr, q, nq, inv64);
     }
 }
 
@@ -286,9 +321,10 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
 // FAST selects the forward schedule without per-butterfly reduction of u (only
 // when the caller needs canonical or multiplied outputs and every q < 2^58).
 // ============================================================================
-template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
+template <int LOG_N, int LOG_E, int ROWS, int MODE, int S>
 __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kernel(NttArgs a) {
     constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E;
+    constexpr bool FAST = S >= 1, FASTI = S >= 2;  // schedules: see kSched* below
     extern __shared__ uint64_t smem_block[];
     const uint32_t tid = threadIdx.x;
     // launch order is limb-major (all polys of limb 0, then limb 1, ...) so that
@@ -366,9 +402,10 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             // inverse's first group (I0::G == 0), so it stays in registers
             static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
         }
-        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr, srptr,
-                                                                  q, nq);
-        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT>(x, sm, tid, 0, itw, sptr, srptr, q, nq);
+        const uint64_t inv64 = FASTI ? a.bar[limb].r1 : 0;
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI, FASTI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr,
+                                                                         srptr, q, nq, inv64);
+        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT, FASTI>(x, sm, tid, 0, itw, sptr, srptr, q, nq, inv64);
         // last group: elements tid + jj*T, coalesced store
         using Last = InvRounds<LOG_N, LOG_E, I0::COUNT - 1>;
         static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
@@ -408,9 +445,10 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
 // other's barrier and exchange phases.
 __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
 __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
     ntt_cluster_kernel(NttArgs a) {
+    constexpr bool FAST = S >= 1, FASTI = S >= 2;  // schedules: see kSched* below
     constexpr int LOG_C = LOG_N - LOG_M;
     constexpr int N = 1 << LOG_N, M = 1 << LOG_M, E = 1 << LOG_E, LOG_T = LOG_M - LOG_E, T = 1 << LOG_T;
     constexpr int LOG_K = LOG_E - LOG_C;  // top block bits handled by the cross phase
@@ -503,9 +541,11 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
             __syncthreads();
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         }
-        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, group_base<LOG_E>(tid, I0::G), rank, itw, nullptr,
-                                                                  nullptr, q, nq);
-        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1>(x, sm, tid, rank, itw, nullptr, nullptr, q, nq);
+        const uint64_t inv64 = FASTI ? a.bar[limb].r1 : 0;
+        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI, FASTI>(x, group_base<LOG_E>(tid, I0::G), rank, itw,
+                                                                         nullptr, nullptr, q, nq, inv64);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1, FASTI>(x, sm, tid, rank, itw, nullptr, nullptr, q, nq,
+                                                                     inv64);
         {
             // last local round: its smem loads precede the cluster arrive, so no
             // CTA overwrites a block that another CTA is still reading
@@ -517,8 +557,8 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
             // release: these shared-memory reads must be performed before any
             // other CTA, released by this barrier, overwrites the block
             cluster_arrive_release();
-            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI>(x, base, rank, itw, nullptr, nullptr, q,
-                                                                               nq);
+            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI, FASTI>(x, base, rank, itw, nullptr,
+                                                                                      nullptr, q, nq, inv64);
             cluster_wait_acquire();
             // element at row index i = rank*M + base + (jj << G) belongs to cross
             // group c = i mod N/E (CTA c >> LOG_T, thread c mod T) as element i >> GX:
@@ -536,7 +576,8 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         // cross inverse stages (the last LOG_E, including the N^-1-scaled one)
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = sm[padi((jj << LOG_T) + tid)];
-        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1>(x, gt, 0, itw, a.inv_n + limb, a.inv_last + limb, q, nq);
+        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1, FASTI>(x, gt, 0, itw, a.inv_n + limb, a.inv_last + limb, q,
+                                                                 nq, inv64);
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
     }
@@ -546,11 +587,20 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
 
 namespace pg {
 
-template <int LOG_N, int LOG_E, int ROWS, int MODE, bool FAST>
+// Butterfly schedules (template parameter S of the kernels).  All return the same
+// canonical values; the faster ones need headroom below 2^64:
+//   kSchedExact    the reference's Harvey / Gentleman-Sande schedule (lazy outputs)
+//   kSchedFastFwd  forward without the u = x mod 2q step: every q < 2^58
+//   kSchedFastBoth also the inverse without the x reduction: every q < 2^50
+constexpr int kSchedExact = 0, kSchedFastFwd = 1, kSchedFastBoth = 2;
+inline bool fast_fwd_ok(const NttArgs& a) { return a.max_modulus < (1ull << 58); }
+inline bool fast_inv_ok(const NttArgs& a) { return a.max_modulus < (1ull << 50); }
+
+template <int LOG_N, int LOG_E, int ROWS, int MODE, int S>
 static int launch_block(const NttArgs& a, cudaStream_t st) {
     constexpr int T = 1 << (LOG_N - LOG_E);
     constexpr size_t smem = (size_t)ROWS * padded(1 << LOG_N) * sizeof(uint64_t);
-    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE, FAST>;
+    auto kern = ntt_block_kernel<LOG_N, LOG_E, ROWS, MODE, S>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_block_kernel: shared memory attribute");
     dim3 block(T, ROWS);
@@ -561,11 +611,11 @@ static int launch_block(const NttArgs& a, cudaStream_t st) {
     return PG_OK;
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, bool FAST>
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
 static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
     constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
-    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, FAST>;
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
     if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");

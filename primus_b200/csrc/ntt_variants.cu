@@ -39,9 +39,9 @@ constexpr VariantInfo kVariants[] = {
 
 template <int MODE>
 int run_variant(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
-    // the forward and the round trip variants run the fast schedule (canonical
-    // outputs, every q < 2^58); the inverse has one schedule
-    constexpr bool F = MODE != MODE_INV;
+    // the variants run the fast schedules: the forward every q < 2^58, the
+    // inverse and the round trip every q < 2^50 (canonical outputs)
+    constexpr int F = MODE == MODE_FWD ? kSchedFastFwd : kSchedFastBoth;
     switch (log_n * 8 + (uint32_t)v) {
         case 10 * 8 + 1: return launch_block<10, 3, 2, MODE, F>(a, st);
         case 10 * 8 + 2: return launch_block<10, 2, 1, MODE, F>(a, st);
@@ -174,14 +174,14 @@ int pg_ntt_autotune(pg_ntt_table* t, size_t polys, pg_ntt_tuning* out) {
     NttArgs a = make_args(t, b.data, rows, 0);
     a.plain = b.plain;
     a.plain_q = b.plain_q;
-    const bool fast = a.max_modulus < (1ull << 58);
+    const bool ffwd = fast_fwd_ok(a), finv = fast_inv_ok(a);
     const int count = ntt_variant_count(t->log_n);
     pg_ntt_tuning res{};
     for (int mode = 0; mode < 3; ++mode) {
         int best = 0;
         float best_us = 0;
-        // without the fast schedule only the inverse has alternative shapes
-        const int vmax = (mode == MODE_INV || fast) ? count : 1;
+        // alternative shapes exist on the fast schedules only
+        const int vmax = (mode == MODE_FWD ? ffwd : finv) ? count : 1;
         for (int v = 0; v < vmax; ++v) {
             float us = 0;
             rc = time_variant(a, t->log_n, mode, v, b.st, b.e0, b.e1, &us);
