@@ -166,27 +166,39 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_reference(moduli, seconds_target=12.0, threads=None):
-    """Time the oracle port of the reference's path (UintNttTable + DcrtPolynomial::mul_assign)
-    on the host cores over a bounded sample of the workload; returns (NTT/s, sample text, threads)."""
+def cpu_reference(moduli, seconds_target=12.0, threads=None, path=None):
+    """Time the reference's CPU path for this workload on the host cores over a bounded
+    sample; returns (NTT/s, sample text, threads).  The path is the one the reference
+    dispatches to (primus_ntt/src/ntt/hexl/mod.rs:473-540): the HEXL-style AVX-512
+    IFMA52 transforms when the host has avx512ifma and q < 2^50 (oracle/hexl_ifma.c),
+    else the scalar UintNttTable restatement.  OpenMP over rows."""
     import oracle as O
     threads = threads or cpu_threads()
     ref = O.DcrtTable(LOG_N, moduli)
     plain = O.uniform_rns(SEED + 7, 0, moduli, N)
     plain = ref.forward(plain)
-    one = O.uniform_rns(SEED, 0, moduli, N)
+    use_hexl = (path or ("hexl" if O.hexl_available() else "scalar")) == "hexl"
+    if use_hexl:
+        hx = O.HexlDcrt(ref)
+        plain_p = hx.prepare(plain)
+        run = lambda x: hx.polymul_roundtrip(x, plain, plain_p, threads=threads)  # noqa: E731
+        label = "HEXL-style AVX-512 IFMA52 restatement of the reference's fastest CPU path"
+    else:
+        run = lambda x: ref.polymul_roundtrip(x, plain, threads=threads)  # noqa: E731
+        label = "C restatement of UintNttTable/DcrtPolynomial (scalar)"
+    one = O.uniform_rns(SEED, 0, moduli, N).ravel().copy()
     t0 = time.perf_counter()
-    ref.polymul_roundtrip(one, plain, threads=threads)
-    t1 = time.perf_counter()
-    per_poly = max(t1 - t0, 1e-4)
+    run(one)
+    per_poly = max(time.perf_counter() - t0, 1e-4)
     # at least one poly per thread so every core works; bounded to ~seconds_target
-    polys = int(max(threads, min(POLYS, seconds_target / per_poly * threads / max(threads, 1))))
+    polys = int(max(threads, min(POLYS, seconds_target / per_poly)))
     polys = max(1, min(POLYS, polys))
-    x = np.concatenate([O.uniform_rns(SEED, p * L, moduli, N) for p in range(polys)])
+    x = np.concatenate([O.uniform_rns(SEED, p * L, moduli, N).ravel() for p in range(polys)])
     t0 = time.perf_counter()
-    ref.polymul_roundtrip(x, plain, threads=threads)
+    run(x)
     dt = time.perf_counter() - t0
-    return 2 * polys / dt, f"{polys} of {POLYS} polys (24 limbs, N=2^16) round trip, {dt:.2f} s", threads
+    return 2 * polys / dt, f"{label}, OpenMP over rows; {polys} of {POLYS} polys (24 limbs, N=2^16) round trip, " \
+                           f"{dt:.2f} s", threads
 
 
 def run_reference(args):
@@ -209,8 +221,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": NTT_PER_STEP / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded uniform residues)", "config": WORKLOAD,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
-                         "sample": "C restatement of UintNttTable/DcrtPolynomial (oracle), OpenMP over rows; " + sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -313,9 +324,12 @@ def run_gpu(args):
         cpu = None
         if world == 1 and not args.no_cpu:
             import oracle as O  # the checker, timed as the CPU baseline only
-            v, sample, thr = cpu_reference(O.ntt_primes(1 << 50, 2 * N, L), seconds_target=args.cpu_seconds)
-            cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-                   "sample": "C restatement of UintNttTable/DcrtPolynomial (oracle), OpenMP over rows; " + sample}
+            moduli = O.ntt_primes(1 << 50, 2 * N, L)
+            v, sample, thr = cpu_reference(moduli, seconds_target=args.cpu_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+            if O.hexl_available():  # the scalar restatement beside it, on a short sample
+                sv, ssample, _ = cpu_reference(moduli, seconds_target=3.0, threads=thr, path="scalar")
+                cpu["scalar_port"] = {"value": sv, "sample": ssample}
         workloads = None
         if world == 1 and not args.no_extra:
             workloads = {"polymul_n1024": bench_polymul_1024(P, stream),

@@ -20,6 +20,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "primus_oracle.c")
+SRCS = [SRC, os.path.join(HERE, "hexl_ifma.c")]
+HDR = os.path.join(HERE, "primus_oracle.h")
 
 u64p = C.POINTER(C.c_uint64)
 u32p = C.POINTER(C.c_uint32)
@@ -28,8 +30,10 @@ u8p = C.POINTER(C.c_uint8)
 
 def build(force: bool = False) -> str:
     """Compile the oracle with gcc (OpenMP for the multi-threaded CPU baseline)."""
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(SRC):
-        cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-fopenmp", "-o", LIB_PATH, SRC, "-lm"]
+    newest = max(os.path.getmtime(f) for f in SRCS + [HDR])
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
+        # hexl_ifma.c marks its AVX-512 functions with target attributes; the rest is x86-64-v3
+        cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-fopenmp", "-o", LIB_PATH, *SRCS, "-lm"]
         subprocess.check_call(cmd)
     return LIB_PATH
 
@@ -122,6 +126,13 @@ def lib():
             "orc_ksk_generate": (None, [C.c_void_p, C.c_uint32, C.c_uint32, u64p, u64p, C.c_uint64, C.c_double, u64p]),
             "orc_glwe_decrypt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, C.c_uint64, C.c_uint64, u64p]),
             "orc_bfv_delta": (None, [C.c_void_p, C.c_uint64, u64p]),
+            "orc_hexl_available": (C.c_int, []),
+            "orc_hexl_table_new": (C.c_void_p, [C.c_void_p]),
+            "orc_hexl_table_delete": (None, [C.c_void_p]),
+            "orc_hexl_forward": (None, [C.c_void_p, u64p]),
+            "orc_hexl_inverse": (None, [C.c_void_p, u64p]),
+            "orc_hexl_precon52": (None, [u64p, u64p, C.c_size_t, C.c_uint64]),
+            "orc_hexl_polymul_roundtrip": (None, [C.c_void_p, C.c_uint32, u64p, u64p, u64p, C.c_size_t, C.c_int]),
             "orc_hybrid_ks_new": (C.c_void_p, [C.c_uint32, u64p, C.c_uint32, C.c_uint32, C.c_uint32]),
             "orc_hybrid_ks_delete": (None, [C.c_void_p]),
             "orc_hybrid_ks_dnum": (C.c_uint32, [C.c_void_p]),
@@ -541,3 +552,55 @@ class HybridKeySwitch:
         out = np.zeros((k_out + 1) * self.L * self.n, np.uint64)
         lib().orc_hybrid_key_switch(self.h, k_in, k_out, p64(u64(key)), p64(u64(c_in)), p64(out))
         return out
+
+
+def hexl_available() -> bool:
+    """True when this host runs the AVX-512 IFMA52 transforms (the reference's HEXL path)."""
+    return bool(lib().orc_hexl_available())
+
+
+class HexlDcrt:
+    """HEXL-style AVX-512 IFMA52 transforms over a DcrtTable's primes (q < 2^50):
+    the reference's fastest CPU path, used as the timed CPU baseline."""
+
+    def __init__(self, table: "DcrtTable"):
+        self.table, self.L, self.n = table, table.L, table.n
+        self.h = []
+        for i in range(table.L):
+            h = lib().orc_hexl_table_new(table._arr[i])
+            if not h:
+                raise ValueError("HEXL path needs q < 2^50 and n >= 16")
+            self.h.append(h)
+        self._harr = (C.c_void_p * table.L)(*self.h)
+
+    def __del__(self):
+        for h in getattr(self, "h", []):
+            lib().orc_hexl_table_delete(h)
+        self.h = []
+
+    def forward(self, a):
+        a = u64(a).copy()
+        for r in range(a.size // self.n):
+            lib().orc_hexl_forward(self.h[r % self.L], p64(a[r * self.n:]))
+        return a
+
+    def inverse(self, a):
+        a = u64(a).copy()
+        for r in range(a.size // self.n):
+            lib().orc_hexl_inverse(self.h[r % self.L], p64(a[r * self.n:]))
+        return a
+
+    def prepare(self, plain):
+        plain = np.ascontiguousarray(u64(plain).ravel())
+        pp = np.zeros_like(plain)
+        for l in range(self.L):
+            lib().orc_hexl_precon52(p64(plain[l * self.n:]), p64(pp[l * self.n:]), self.n, self.table.moduli[l])
+        return pp
+
+    def polymul_roundtrip(self, a, plain, plain_p, threads=1):
+        """In place on a: forward, x plain (NTT domain, quotients from prepare), inverse."""
+        plain = np.ascontiguousarray(u64(plain).ravel())
+        plain_p = np.ascontiguousarray(u64(plain_p).ravel())
+        lib().orc_hexl_polymul_roundtrip(self._harr, self.L, p64(a), p64(plain), p64(plain_p),
+                                         a.size // (self.L * self.n), threads)
+        return a

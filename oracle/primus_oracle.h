@@ -287,6 +287,18 @@ void orc_hybrid_ks_factor(const orc_hybrid_ks *h, uint32_t g, uint64_t *fac);
 void orc_hybrid_key_switch(const orc_hybrid_ks *h, uint32_t k_in, uint32_t k_out, const uint64_t *key,
                            const uint64_t *c_in, uint64_t *c_out);
 
+/* ---- HEXL-style AVX-512 IFMA52 transforms (hexl_ifma.c): the reference's fastest
+ * CPU path, timed as the CPU baseline (q < 2^50, n >= 16, host with avx512ifma) */
+typedef struct orc_hexl_table orc_hexl_table;
+int orc_hexl_available(void);
+orc_hexl_table *orc_hexl_table_new(const orc_ntt_table *t); /* NULL if q >= 2^50 or n < 16 */
+void orc_hexl_table_delete(orc_hexl_table *h);
+void orc_hexl_forward(const orc_hexl_table *h, uint64_t *a); /* canonical in and out */
+void orc_hexl_inverse(const orc_hexl_table *h, uint64_t *a); /* [0, 2q) in, canonical out */
+void orc_hexl_precon52(const uint64_t *y, uint64_t *yp, size_t n, uint64_t q);
+void orc_hexl_polymul_roundtrip(orc_hexl_table *const *tables, uint32_t L, uint64_t *a, const uint64_t *plain,
+                                const uint64_t *plain_p, size_t polys, int threads);
+
 #ifdef __cplusplus
 }
 #endif
