@@ -299,18 +299,20 @@ def run_gpu(args):
     nat.call("pg_host_alloc", C.byref(hp), nbytes)
     host = np.ctypeslib.as_array((C.c_uint64 * (POLYS * L * N)).from_address(hp.value))
     host[:] = data.numpy()
+
+    def e2e_step():
+        # the reference-facing call on a host slice: copies in, fused launches and
+        # copies out pipelined over chunks inside the library (synchronous)
+        nat.call("pg_dcrt_polymul_ntt_plain_host", tab.h, hp.value, plain.ptr, plain_q.ptr, POLYS, stream.h)
+
     for _ in range(2):
-        nat.call("pg_memcpy_h2d", data.ptr, hp.value, nbytes, stream.h)
-        step()
-        nat.call("pg_memcpy_d2h", hp.value, data.ptr, nbytes, stream.h)
+        e2e_step()
     stream.synchronize()
     e2e_steps = max(3, min(args.steps, 10))
     dist_barrier(dist)
     e0.record(stream)
     for _ in range(e2e_steps):
-        nat.call("pg_memcpy_h2d", data.ptr, hp.value, nbytes, stream.h)
-        step()
-        nat.call("pg_memcpy_d2h", hp.value, data.ptr, nbytes, stream.h)
+        e2e_step()
     e1.record(stream)
     stream.synchronize()
     e2e_ms = dist_max(dist, e0.elapsed_ms(e1) / e2e_steps, local)
@@ -348,7 +350,7 @@ def run_gpu(args):
                                                     for k in ('forward', 'inverse', 'round_trip')) + ")"),
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                    "ms_per_step": e2e_ms, "path": "pg_memcpy_h2d -> pg_dcrt_polymul_ntt_plain -> pg_memcpy_d2h"},
+                    "ms_per_step": e2e_ms, "path": "pg_dcrt_polymul_ntt_plain_host (pinned host slice; chunked H2D / fused launch / D2H on 3 streams)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,

@@ -154,7 +154,9 @@ int pg_ntt_forward(const pg_ntt_table *table, uint64_t *d_data, size_t polys, in
 int pg_ntt_inverse(const pg_ntt_table *table, uint64_t *d_data, size_t polys, int lazy,
                    void *stream);
 /* Host-slice forms with the reference's exact call semantics (copy in,
- * transform, copy out, synchronous). */
+ * transform, copy out, synchronous).  Large slices run as a pipeline of
+ * chunks on three streams, so copies in, transforms and copies out overlap
+ * when the host memory is pinned (pg_host_alloc). */
 int pg_ntt_forward_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
 int pg_ntt_inverse_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
 /* NTT of coeff*X^degree into every limb (coeff < every q), of X^degree and of
@@ -215,6 +217,14 @@ int pg_dcrt_mul_prepared(const pg_ntt_table *table, uint64_t *d_x, const uint64_
 int pg_dcrt_polymul_ntt_plain(const pg_ntt_table *table, uint64_t *d_data,
                               const uint64_t *d_plain, const uint64_t *d_plain_q, size_t polys,
                               void *stream);
+/* The same on a host slice [polys][L][N] in place (the plaintext stays resident
+ * on the device): the reference's three calls on &mut [u64], through the
+ * pipelined host path of pg_ntt_forward_host.  Synchronous; the pipeline runs
+ * after the work already on `stream` and `stream` is ordered after it (NULL: no
+ * ordering with other streams). */
+int pg_dcrt_polymul_ntt_plain_host(const pg_ntt_table *table, uint64_t *h_data,
+                                   const uint64_t *d_plain, const uint64_t *d_plain_q, size_t polys,
+                                   void *stream);
 
 /* ------------------------------------------------------------- RNS base
  * RNSBase (primus_rns/src/base.rs:24-90): moduli, Q = prod q_i as a BigUint of

@@ -325,24 +325,76 @@ static int check_table_data(const pg_ntt_table* t, const void* d, size_t polys) 
     return PG_OK;
 }
 
-static int host_roundtrip(const pg_ntt_table* t, uint64_t* h, size_t polys, int lazy, int mode) {
+// Host slices through a copy / compute pipeline: chunks of whole polys are
+// copied in on one of kPipeStreams streams, transformed there and copied back,
+// so that the two copy engines (host->device and device->host) and the SMs work
+// at the same time.  With pinned host memory the copies overlap; with pageable
+// memory the same calls run at the speed of the driver's staged copies.
+// Synchronous, like the reference's &mut [u64] calls.
+static int host_pipeline(const pg_ntt_table* t, uint64_t* h, size_t polys, int lazy, int mode,
+                         const uint64_t* d_plain, const uint64_t* d_plain_q, cudaStream_t user = nullptr) {
     int rc = check_table_data(t, h, polys);
     if (rc) return rc;
     if (polys == 0) return PG_OK;
-    const size_t bytes = polys * t->L * t->n * sizeof(uint64_t);
-    uint64_t* d = nullptr;
-    PG_CUDA(cudaMalloc(&d, bytes));
-    cudaError_t e = cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        cudaFree(d);
-        return cuda_status(e, "host transform: copy in");
+    constexpr int kPipeStreams = 3;
+    constexpr size_t kChunkBytes = 64ull << 20;
+    const size_t poly_words = (size_t)t->L * t->n;
+    const size_t chunk = std::max<size_t>(1, kChunkBytes / (poly_words * sizeof(uint64_t)));
+    const size_t nchunks = (polys + chunk - 1) / chunk;
+    const int ns = (int)std::min<size_t>(kPipeStreams, nchunks);
+    cudaStream_t st[kPipeStreams] = {};
+    cudaEvent_t ev[kPipeStreams + 1] = {};
+    for (int i = 0; i < ns; ++i) PG_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
+    for (int i = 0; i <= ns && user; ++i) PG_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    if (user) {  // the pipeline starts after the caller's stream and rejoins it at the end
+        PG_CUDA(cudaEventRecord(ev[ns], user));
+        for (int i = 0; i < ns; ++i) PG_CUDA(cudaStreamWaitEvent(st[i], ev[ns], 0));
     }
-    rc = launch_ntt(make_args(t, d, polys * t->L, lazy), t->log_n, mode, 0);
-    if (rc == PG_OK) {
-        e = cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost);
+    auto cleanup = [&](void* buf) {
+        for (int i = 0; i < ns && user; ++i) {
+            cudaEventRecord(ev[i], st[i]);
+            cudaStreamWaitEvent(user, ev[i], 0);
+        }
+        for (int i = 0; i < ns; ++i) cudaStreamSynchronize(st[i]);
+        if (buf) {
+            scratch_free(buf, st[0]);
+            cudaStreamSynchronize(st[0]);
+        }
+        for (int i = 0; i < ns; ++i) cudaStreamDestroy(st[i]);
+        for (int i = 0; i <= ns; ++i)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+    };
+    void* buf = nullptr;
+    cudaError_t e = scratch_alloc(&buf, (size_t)ns * chunk * poly_words * sizeof(uint64_t), st[0]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st[0]);
+    if (e != cudaSuccess) {
+        cleanup(nullptr);
+        return cuda_status(e, "host transform: staging buffers");
+    }
+    for (size_t c = 0; c < nchunks && rc == PG_OK; ++c) {
+        const int si = (int)(c % ns);
+        const size_t p0 = c * chunk, np = std::min(chunk, polys - p0);
+        uint64_t* d = (uint64_t*)buf + (size_t)si * chunk * poly_words;
+        uint64_t* hp = h + p0 * poly_words;
+        const size_t bytes = np * poly_words * sizeof(uint64_t);
+        e = cudaMemcpyAsync(d, hp, bytes, cudaMemcpyHostToDevice, st[si]);
+        if (e != cudaSuccess) {
+            rc = cuda_status(e, "host transform: copy in");
+            break;
+        }
+        NttArgs a = make_args(t, d, np * t->L, lazy);
+        a.plain = d_plain;
+        a.plain_q = d_plain_q;
+        rc = launch_ntt(a, t->log_n, mode, st[si]);
+        if (rc) break;
+        e = cudaMemcpyAsync(hp, d, bytes, cudaMemcpyDeviceToHost, st[si]);
         if (e != cudaSuccess) rc = cuda_status(e, "host transform: copy out");
     }
-    cudaFree(d);
+    cleanup(buf);
+    if (rc == PG_OK) {
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_status(e, "host transform");
+    }
     return rc;
 }
 
@@ -365,11 +417,11 @@ int pg_ntt_inverse(const pg_ntt_table* t, uint64_t* d_data, size_t polys, int la
 }
 
 int pg_ntt_forward_host(const pg_ntt_table* t, uint64_t* h_data, size_t polys, int lazy) {
-    return host_roundtrip(t, h_data, polys, lazy, MODE_FWD);
+    return host_pipeline(t, h_data, polys, lazy, MODE_FWD, nullptr, nullptr);
 }
 
 int pg_ntt_inverse_host(const pg_ntt_table* t, uint64_t* h_data, size_t polys, int lazy) {
-    return host_roundtrip(t, h_data, polys, lazy, MODE_INV);
+    return host_pipeline(t, h_data, polys, lazy, MODE_INV, nullptr, nullptr);
 }
 
 int pg_ntt_monomial(const pg_ntt_table* t, uint64_t coeff, size_t degree, uint64_t* d_out, void* stream) {
@@ -393,6 +445,12 @@ int pg_dcrt_polymul_ntt_plain(const pg_ntt_table* t, uint64_t* d_data, const uin
     a.plain = d_plain;
     a.plain_q = d_plain_q;
     return launch_ntt(a, t->log_n, MODE_RT, (cudaStream_t)stream);
+}
+
+int pg_dcrt_polymul_ntt_plain_host(const pg_ntt_table* t, uint64_t* h_data, const uint64_t* d_plain,
+                                   const uint64_t* d_plain_q, size_t polys, void* stream) {
+    if (!d_plain || !d_plain_q) return set_error(PG_ERR_INVALID_ARGUMENT, "plaintext is NULL");
+    return host_pipeline(t, h_data, polys, 0, MODE_RT, d_plain, d_plain_q, (cudaStream_t)stream);
 }
 
 }  // extern "C"

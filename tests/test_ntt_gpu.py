@@ -143,6 +143,46 @@ def test_host_slice_dropin_lazy(gpu):
         tab.transform_slice(np.zeros(1000, np.uint64))
 
 
+def test_host_slices_pipelined(gpu):
+    # 5 polys of 24 limbs at N = 2^16 (25 MB each): three chunks on the three
+    # pipeline streams, in pinned and in pageable host memory
+    import ctypes as C
+    from primus_b200 import _native as nat
+    log_n, L, polys = 16, 24, 5
+    n = 1 << log_n
+    moduli = O.ntt_primes(1 << 50, 2 * n, L)
+    tab = gpu.DcrtTable(log_n, moduli)
+    d = gpu.DeviceBuffer(polys * L * n)
+    tab.fill_uniform(d, polys, seed=0x9A)
+    x = d.numpy()
+    plain = gpu.DeviceBuffer(L * n)
+    tab.fill_uniform(plain, 1, seed=0x9B)
+    plain_q = gpu.DeviceBuffer(L * n)
+    tab.shoup_prepare(plain, plain_q, 1)
+    want_fwd = gpu.DeviceBuffer.from_numpy(x)
+    tab.forward(want_fwd, polys)
+    want_rt = gpu.DeviceBuffer.from_numpy(x)
+    tab.polymul_ntt_plain(want_rt, plain, plain_q, polys)
+    gpu.synchronize()
+    # pageable
+    y = x.copy()
+    tab.transform_slice(y)
+    assert np.array_equal(y, want_fwd.numpy())
+    tab.inverse_transform_slice(y)
+    assert np.array_equal(y, x)
+    # pinned, fused round trip on the caller's stream
+    hp = C.c_void_p()
+    nat.call("pg_host_alloc", C.byref(hp), x.nbytes)
+    try:
+        host = np.ctypeslib.as_array((C.c_uint64 * x.size).from_address(hp.value))
+        host[:] = x
+        st = gpu.Stream()
+        nat.call("pg_dcrt_polymul_ntt_plain_host", tab.h, hp.value, plain.ptr, plain_q.ptr, polys, st.h)
+        assert np.array_equal(host, want_rt.numpy())
+    finally:
+        nat.call("pg_host_free", hp.value)
+
+
 @pytest.mark.parametrize("log_n", [1, 6, 11, 16])
 def test_monomials(gpu, log_n):
     n = 1 << log_n
