@@ -329,6 +329,19 @@ int pg_key_switch(const pg_ntt_table *table, const pg_gadget_basis *basis, uint3
                   uint32_t k_out, const uint64_t *d_key, const uint64_t *d_c_in,
                   uint64_t *d_c_out, size_t batch, void *d_workspace, size_t workspace_bytes,
                   void *stream);
+/* GLWE automorphism X -> X^degree (degree odd) in the NTT domain:
+ * DcrtGlweAutoKey::automorphism_inplace (primus_fhe_core/src/automorphism/glwe/dcrt.rs:269-331).
+ * Every poly of each ciphertext is permuted in the NTT domain
+ * (generate_ntt_permutation, :43-63), the k masks are inverse-transformed and
+ * key-switched with the automorphism key, the permuted body is added:
+ * c_out = -(sum_i key_i (x) sigma(a_i)) + (0, .., sigma(b)).  c_in, c_out:
+ * [batch][k+1][L][N] NTT domain (must not overlap); key: k GLevs
+ * [k][d][k+1][L][N] (GLev of sigma(s_i) under s, NTT domain). */
+size_t pg_glwe_automorphism_workspace_size(const pg_ntt_table *table, const pg_gadget_basis *basis,
+                                           uint32_t k, size_t batch);
+int pg_glwe_automorphism(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                         uint64_t degree, const uint64_t *d_key, const uint64_t *d_c_in, uint64_t *d_c_out,
+                         size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
 /* pg_ext_product for callers that cannot allocate device memory when they
  * call (hosts holding only device pointers owned by another runtime, serving
  * processes that reserve HBM at start-up and forbid later allocations).  No

@@ -126,6 +126,8 @@ def lib():
             "orc_ksk_generate": (None, [C.c_void_p, C.c_uint32, C.c_uint32, u64p, u64p, C.c_uint64, C.c_double, u64p]),
             "orc_glwe_decrypt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, C.c_uint64, C.c_uint64, u64p]),
             "orc_bfv_delta": (None, [C.c_void_p, C.c_uint64, u64p]),
+            "orc_ntt_auto_perm": (None, [C.c_uint32, C.c_uint64, u32p]),
+            "orc_glwe_automorphism": (None, [C.c_void_p, C.c_uint32, C.c_uint64, u64p, u64p, u64p]),
             "orc_hexl_available": (C.c_int, []),
             "orc_hexl_table_new": (C.c_void_p, [C.c_void_p]),
             "orc_hexl_table_delete": (None, [C.c_void_p]),
@@ -490,6 +492,12 @@ class Lattice:
         lib().orc_key_switch(self.pctx, k_in, k_out, p64(u64(key)), p64(u64(c_in)), p64(out))
         return out
 
+    def automorphism(self, k, degree, key, ct_in):
+        """DcrtGlweAutoKey::automorphism_inplace: NTT-domain GLWE in and out."""
+        out = np.zeros((k + 1) * self.L * self.n, np.uint64)
+        lib().orc_glwe_automorphism(self.pctx, k, degree, p64(u64(key)), p64(u64(ct_in)), p64(out))
+        return out
+
     def ternary(self, seed, stream):
         out = np.zeros(self.L * self.n, np.uint64)
         lib().orc_sample_ternary(seed, stream, p64(u64(self.table.moduli)), self.L, self.n, p64(out))
@@ -604,3 +612,10 @@ class HexlDcrt:
         lib().orc_hexl_polymul_roundtrip(self._harr, self.L, p64(a), p64(plain), p64(plain_p),
                                          a.size // (self.L * self.n), threads)
         return a
+
+
+def ntt_auto_perm(log_n: int, degree: int) -> np.ndarray:
+    """generate_ntt_permutation: out[d] = in[perm[d]] in bit-reversed NTT storage."""
+    perm = np.zeros(1 << log_n, np.uint32)
+    lib().orc_ntt_auto_perm(log_n, degree, perm.ctypes.data_as(u32p))
+    return perm

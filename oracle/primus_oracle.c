@@ -1518,3 +1518,53 @@ void orc_hybrid_key_switch(const orc_hybrid_ks *h, uint32_t k_in, uint32_t k_out
     free(ext);
     free(conv);
 }
+
+/* ======================================================================
+ * NTT-domain automorphism (primus_fhe_core/src/automorphism/glwe/dcrt.rs)
+ * ====================================================================== */
+/* generate_ntt_permutation (:43-63): natural index i holds the evaluation at
+ * psi^(2i+1); sigma_k moves it to psi^(k(2i+1) mod 2N), index (j-1)/2; both in
+ * bit-reversed storage */
+void orc_ntt_auto_perm(uint32_t log_n, uint64_t degree, uint32_t *perm) {
+    const uint64_t n = 1ull << log_n, mask = 2 * n - 1;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t j = (degree * (2 * i + 1)) & mask;
+        const uint64_t target = (j - 1) / 2;
+        perm[rev_bits((uint32_t)i, log_n)] = rev_bits((uint32_t)target, log_n);
+    }
+}
+
+/* automorphism_inplace (:269-331): for each a_i: permute, inverse NTT, GLev MAC
+ * into the result; then result = (-a', sigma(b) - b') */
+void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree, const uint64_t *key,
+                           const uint64_t *ct_in, uint64_t *ct_out) {
+    const size_t n = c->n;
+    const uint32_t L = c->L, log_n = (uint32_t)__builtin_ctzll(n);
+    const size_t poly = (size_t)L * n;
+    const size_t glev = (size_t)c->basis->decompose_length * (k + 1) * poly;
+    uint32_t *perm = malloc(n * sizeof(uint32_t));
+    orc_ntt_auto_perm(log_n, degree, perm);
+    uint64_t *tmp = malloc(poly * 8);
+    memset(ct_out, 0, (size_t)(k + 1) * poly * 8);
+    for (uint32_t i = 0; i < k; ++i) {
+        const uint64_t *a = ct_in + (size_t)i * poly;
+        for (uint32_t l = 0; l < L; ++l)
+            for (size_t d = 0; d < n; ++d) tmp[(size_t)l * n + d] = a[(size_t)l * n + perm[d]];
+        for (uint32_t l = 0; l < L; ++l) orc_ntt_inverse(c->tables[l], tmp + (size_t)l * n);
+        orc_glev_mac_crt_poly(c, k, ct_out, key + (size_t)i * glev, tmp);
+    }
+    const uint64_t *b = ct_in + (size_t)k * poly;
+    for (uint32_t l = 0; l < L; ++l)
+        for (size_t d = 0; d < n; ++d) tmp[(size_t)l * n + d] = b[(size_t)l * n + perm[d]];
+    for (uint32_t i = 0; i < k; ++i)
+        for (uint32_t l = 0; l < L; ++l) orc_neg_assign(ct_out + (size_t)i * poly + (size_t)l * n, n, c->tables[l]->q);
+    /* sub_to_right: b_out = sigma(b) - b_out */
+    for (uint32_t l = 0; l < L; ++l) {
+        const uint64_t q = c->tables[l]->q;
+        uint64_t *bo = ct_out + (size_t)k * poly + (size_t)l * n;
+        const uint64_t *sb = tmp + (size_t)l * n;
+        for (size_t x = 0; x < n; ++x) bo[x] = sb[x] >= bo[x] ? sb[x] - bo[x] : sb[x] + q - bo[x];
+    }
+    free(tmp);
+    free(perm);
+}

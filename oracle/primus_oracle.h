@@ -287,6 +287,14 @@ void orc_hybrid_ks_factor(const orc_hybrid_ks *h, uint32_t g, uint64_t *fac);
 void orc_hybrid_key_switch(const orc_hybrid_ks *h, uint32_t k_in, uint32_t k_out, const uint64_t *key,
                            const uint64_t *c_in, uint64_t *c_out);
 
+/* ---- NTT-domain automorphism x -> x^degree (primus_fhe_core/src/automorphism/glwe/dcrt.rs) */
+/* generate_ntt_permutation (:43-63): out[d] = in[perm[d]] in bit-reversed storage */
+void orc_ntt_auto_perm(uint32_t log_n, uint64_t degree, uint32_t *perm);
+/* DcrtGlweAutoKey::automorphism_inplace (:269-331): ct_in, ct_out [k+1][L][N] NTT
+ * domain; key = k GLevs [k][d][k+1][L][N] (GLev of sigma(s_i) under s) */
+void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree, const uint64_t *key,
+                           const uint64_t *ct_in, uint64_t *ct_out);
+
 /* ---- HEXL-style AVX-512 IFMA52 transforms (hexl_ifma.c): the reference's fastest
  * CPU path, timed as the CPU baseline (q < 2^50, n >= 16, host with avx512ifma) */
 typedef struct orc_hexl_table orc_hexl_table;

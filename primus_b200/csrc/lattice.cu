@@ -147,6 +147,32 @@ __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
     }
 }
 
+// NTT-domain automorphism X -> X^degree (generate_ntt_permutation,
+// primus_fhe_core/src/automorphism/glwe/dcrt.rs:43-63): bit-reversed slot d
+// holds the evaluation at psi^(2 rev(d) + 1); the result's slot d takes the
+// input's slot rev(((degree (2 rev(d) + 1) mod 2N) - 1) / 2).  Grid: y over the
+// (k+1) polys of each ciphertext, x over their L*N residues; the k masks go to
+// out_a, the body to out_b.
+__global__ void __launch_bounds__(256) auto_perm_kernel(const uint64_t* __restrict__ in, uint64_t* out_a,
+                                                        uint64_t* out_b, size_t batch, uint32_t k, uint32_t L,
+                                                        uint32_t log_n, uint64_t degree) {
+    const uint32_t N = 1u << log_n, LN = L << log_n;
+    const size_t outer = batch * (k + 1);
+    for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const size_t b = o / (k + 1);
+        const uint32_t c = (uint32_t)(o % (k + 1));
+        const uint64_t* src = in + o * LN;
+        uint64_t* dst = c < k ? out_a + (b * k + c) * LN : out_b + b * LN;
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
+            const uint32_t d = lx & (N - 1);
+            const uint32_t i = __brev(d) >> (32 - log_n);
+            const uint64_t j = (degree * (2ull * i + 1)) & (2ull * N - 1);
+            const uint32_t from = __brev((uint32_t)((j - 1) >> 1)) >> (32 - log_n);
+            dst[lx] = src[(lx - d) + from];
+        }
+    }
+}
+
 unsigned grid_for(size_t work, unsigned threads) {
     const size_t cap = 148ull * 2048 / threads;
     size_t b = (work + threads - 1) / threads;
@@ -419,6 +445,46 @@ int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in
     if (rc) return rc;
     // c_out = -(sum_i GLev_i (x) a_i) + (0, .., NTT(b))  (key_switch.rs:96-127)
     return launch_mac(t, gadget_d(g), d_out, nullptr, bt, d_key, dig, batch, k_in, k_out + 1, 1, st);
+}
+
+size_t pg_glwe_automorphism_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k,
+                                           size_t batch) {
+    if (!t || !g) return 0;
+    return ws_bytes(t, g, batch * k, batch * (k + 1) * (size_t)t->L * t->n);
+}
+
+// DcrtGlweAutoKey::automorphism_inplace (primus_fhe_core/src/automorphism/glwe/dcrt.rs:269-331):
+// permute every poly in the NTT domain, inverse-transform the masks, then the
+// key-switch MAC with the permuted body added on the last output poly:
+// c_out = -(sum_i key_i (x) sigma(a_i)) + (0, .., sigma(b)).
+int pg_glwe_automorphism(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, uint64_t degree,
+                         const uint64_t* d_key, const uint64_t* d_in, uint64_t* d_out, size_t batch, void* d_ws,
+                         size_t ws_size, void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (batch == 0) return PG_OK;
+    if (!d_key || !d_in || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (k == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k must be at least 1");
+    if ((degree & 1) == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "automorphism degree must be odd");
+    if (d_in == d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "input and output must not overlap");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t LN = (size_t)t->L * t->n;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, pg_glwe_automorphism_workspace_size(t, g, k, batch), st);
+    if (rc) return rc;
+    uint64_t* pa = (uint64_t*)w.ptr;        // [batch][k][L][N] permuted masks
+    uint64_t* pb = pa + batch * k * LN;     // [batch][L][N] permuted bodies
+    uint64_t* ws = pb + batch * LN;         // digits pipeline scratch
+    auto_perm_kernel<<<grid2(LN, batch * (k + 1)), 256, 0, st>>>(d_in, pa, pb, batch, k, t->L, t->log_n,
+                                                                 degree & (2 * t->n - 1));
+    count_launch();
+    PG_LAUNCH_CHECK("auto_perm_kernel launch");
+    rc = launch_ntt(make_args(t, pa, batch * k * t->L, 0), t->log_n, MODE_INV, st);
+    if (rc) return rc;
+    uint64_t* dig = nullptr;
+    rc = digits_pipeline(t, g, pa, true, batch * k, k, (size_t)k * LN, ws, &dig, st);
+    if (rc) return rc;
+    return launch_mac(t, gadget_d(g), d_out, nullptr, pb, d_key, dig, batch, k, k + 1, 1, st);
 }
 
 // Same computation and outputs as pg_ext_product, with its scratch in the

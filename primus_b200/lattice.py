@@ -152,6 +152,15 @@ def key_switch_workspace_size(table, basis: GadgetBasis, k_in: int, k_out: int, 
     return int(nat.lib().pg_key_switch_workspace_size(table.h, basis.h, k_in, k_out, batch))
 
 
+def glwe_automorphism(table, basis: GadgetBasis, k: int, degree: int, key: DeviceBuffer, c_in: DeviceBuffer,
+                      c_out: DeviceBuffer, batch: int, workspace: DeviceBuffer | None = None, stream=None):
+    """DcrtGlweAutoKey::automorphism_inplace on device buffers (NTT domain)."""
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_glwe_automorphism", table.h, basis.h, k, degree, key.ptr, c_in.ptr, c_out.ptr, batch, ws, wsb,
+         _sh(stream))
+
+
 def glev_mac_crt_poly(table, basis: GadgetBasis, k: int, acc: DeviceBuffer, glev: DeviceBuffer,
                       crt_poly: DeviceBuffer, stream=None):
     call("pg_glev_mac_crt_poly", table.h, basis.h, k, acc.ptr, glev.ptr, crt_poly.ptr, None, 0, _sh(stream))

@@ -262,3 +262,31 @@ def test_fast_convert_matches_crt():
             if all(int(y[j, c]) == (val + alpha * Q) % p for j, p in enumerate(ps)):
                 ok = True
         assert ok
+
+
+def test_automorphism_decrypts_to_permuted_message():
+    # DcrtGlweAutoKey (primus_fhe_core/src/automorphism/glwe/dcrt.rs): decrypting the
+    # automorphism of an encryption of m gives m(X^degree) mod X^N + 1
+    log_n, k, t, gamma = 9, 1, 16, 257
+    n = 1 << log_n
+    moduli = O.ntt_primes(1 << 50, 2 * n, 2)
+    tab = O.DcrtTable(log_n, moduli)
+    base = O.RnsBase(moduli)
+    lat = O.Lattice(tab, base, O.GadgetBasis(base, 20))
+    sk = lat.ternary(3, 10)
+    sk_ntt = tab.forward(sk.copy())
+    for degree in (3, 2 * n - 1, 257):
+        perm = O.ntt_auto_perm(log_n, degree)
+        s_auto = tab.inverse(np.concatenate([sk_ntt.reshape(2, n)[l][perm] for l in range(2)]))
+        key = lat.ksk(k, k, s_auto, sk_ntt, 5 + degree)
+        msg = O.uniform(41, degree, t, n)
+        ct = lat.encrypt(k, sk_ntt, base.wrapping_decompose_small(msg, t), lat.delta(t), 9)
+        m = lat.decrypt(k, sk_ntt, lat.automorphism(k, degree, key, ct), t, gamma)
+        exp = np.zeros(n, np.int64)
+        for i in range(n):
+            j = (i * degree) % (2 * n)
+            if j < n:
+                exp[j] = (exp[j] + int(msg[i])) % t
+            else:
+                exp[j - n] = (exp[j - n] - int(msg[i])) % t
+        assert np.array_equal(m, exp.astype(np.uint64)), degree
