@@ -342,6 +342,23 @@ size_t pg_glwe_automorphism_workspace_size(const pg_ntt_table *table, const pg_g
 int pg_glwe_automorphism(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
                          uint64_t degree, const uint64_t *d_key, const uint64_t *d_c_in, uint64_t *d_c_out,
                          size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
+/* BFV-style GLWE decryption through fast base conversion:
+ * DcrtGlweSecretKey::decrypt_inplace (primus_fhe_core/src/secret_key/glwe.rs:782-837).
+ * phase = b - sum a_i s_i (NTT domain), inverse NTT, x [t gamma]_q, fast
+ * conversion to {t, gamma} (converter.rs:147-175), x -Q^-1, gamma correction.
+ * The decryptor holds the per-limb constants for one table, plaintext modulus t
+ * and correction modulus gamma (t < gamma < 2^62, pairwise coprime with the
+ * moduli: PG_ERR_NOT_COPRIME otherwise).  sk: [k][L][N] NTT domain; ct:
+ * [batch][k+1][L][N] NTT domain; msg out: [batch][N] values in [0, t). */
+typedef struct pg_bfv_decryptor pg_bfv_decryptor;
+int pg_bfv_decryptor_create(const pg_ntt_table *table, uint64_t plain_modulus, uint64_t gamma,
+                            pg_bfv_decryptor **out);
+int pg_bfv_decryptor_destroy(pg_bfv_decryptor *decryptor);
+size_t pg_bfv_decrypt_workspace_size(const pg_bfv_decryptor *decryptor, size_t batch);
+int pg_bfv_decrypt(const pg_bfv_decryptor *decryptor, uint32_t k, const uint64_t *d_sk_ntt,
+                   const uint64_t *d_ct, uint64_t *d_msg, size_t batch, void *d_workspace,
+                   size_t workspace_bytes, void *stream);
+
 /* pg_ext_product for callers that cannot allocate device memory when they
  * call (hosts holding only device pointers owned by another runtime, serving
  * processes that reserve HBM at start-up and forbid later allocations).  No

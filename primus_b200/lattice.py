@@ -209,3 +209,31 @@ class HybridKeySwitch:
             self.close()
         except Exception:
             pass
+
+
+class BfvDecryptor:
+    """BFV decryption through fast base conversion on the device
+    (DcrtGlweSecretKey::decrypt_inplace); pg_bfv_decryptor_* / pg_bfv_decrypt."""
+
+    def __init__(self, table, plain_modulus: int, gamma: int):
+        h = C.c_void_p()
+        call("pg_bfv_decryptor_create", table.h, plain_modulus, gamma, C.byref(h))
+        self.h = h.value
+        self.table, self.t, self.gamma = table, plain_modulus, gamma
+
+    def decrypt(self, k: int, sk_ntt: DeviceBuffer, ct: DeviceBuffer, msg: DeviceBuffer, batch: int,
+                workspace: DeviceBuffer | None = None, stream=None):
+        ws = workspace.ptr if workspace is not None else None
+        wsb = workspace.count * 8 if workspace is not None else 0
+        call("pg_bfv_decrypt", self.h, k, sk_ntt.ptr, ct.ptr, msg.ptr, batch, ws, wsb, _sh(stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_bfv_decryptor_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
