@@ -359,6 +359,24 @@ int pg_bfv_decrypt(const pg_bfv_decryptor *decryptor, uint32_t k, const uint64_t
                    const uint64_t *d_ct, uint64_t *d_msg, size_t batch, void *d_workspace,
                    size_t workspace_bytes, void *stream);
 
+/* Secret-key GLWE encryption on the device: DcrtGlweSecretKey::encrypt_inplace
+ * (primus_fhe_core/src/secret_key/glwe.rs:386-424); with a gadget factor as
+ * `scale` the rows of a GLev / key-switching key (:683-708).  Samplers are pure
+ * functions of (seed, stream, index), identical in the oracle:
+ *   mask a_i limb l of ciphertext j: uniform below q_l, stream stream0 + (j k + i) L + l
+ *   noise of ciphertext j: discrete Gaussian (sigma, bound ceil(24 sigma)) by a
+ *   cumulative table, stream stream0 + 2^32 + j
+ *   b = NTT(e + scale_l * msg) + sum_i a_i s_i
+ * sk: [k][L][N] NTT domain; msg: [batch][L][N] residues in coefficient form, or
+ * NULL for encryptions of zero; h_scale: [L] host values below each q_l (e.g.
+ * Delta = round(Q/t) mod q_l); ct out: [batch][k+1][L][N] NTT domain. */
+typedef struct pg_glwe_encryptor pg_glwe_encryptor;
+int pg_glwe_encryptor_create(const pg_ntt_table *table, double sigma, pg_glwe_encryptor **out);
+int pg_glwe_encryptor_destroy(pg_glwe_encryptor *encryptor);
+int pg_glwe_encrypt(const pg_glwe_encryptor *encryptor, uint32_t k, const uint64_t *d_sk_ntt,
+                    const uint64_t *d_msg, const uint64_t *h_scale, uint64_t seed, uint64_t stream0,
+                    uint64_t *d_ct, size_t batch, void *stream);
+
 /* pg_ext_product for callers that cannot allocate device memory when they
  * call (hosts holding only device pointers owned by another runtime, serving
  * processes that reserve HBM at start-up and forbid later allocations).  No

@@ -128,6 +128,10 @@ def lib():
             "orc_bfv_delta": (None, [C.c_void_p, C.c_uint64, u64p]),
             "orc_ntt_auto_perm": (None, [C.c_uint32, C.c_uint64, u32p]),
             "orc_glwe_automorphism": (None, [C.c_void_p, C.c_uint32, C.c_uint64, u64p, u64p, u64p]),
+            "orc_cdt_table": (C.c_uint32, [C.c_double, u64p, C.c_uint32]),
+            "orc_cdt_sample": (C.c_int64, [u64p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
+            "orc_glwe_encrypt_cdt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, u64p, C.c_double, C.c_uint64,
+                                            C.c_uint64, C.c_uint64, u64p]),
             "orc_hexl_available": (C.c_int, []),
             "orc_hexl_table_new": (C.c_void_p, [C.c_void_p]),
             "orc_hexl_table_delete": (None, [C.c_void_p]),
@@ -497,6 +501,14 @@ class Lattice:
         out = np.zeros((k + 1) * self.L * self.n, np.uint64)
         lib().orc_glwe_automorphism(self.pctx, k, degree, p64(u64(key)), p64(u64(ct_in)), p64(out))
         return out
+
+    def encrypt_cdt(self, k, sk_ntt, msg, scale, seed, stream0, index, sigma=3.2):
+        """GLWE encryption with the CDT Gaussian sampler (ciphertext `index` of a batch)."""
+        ct = np.zeros((k + 1) * self.L * self.n, np.uint64)
+        mp = p64(u64(msg)) if msg is not None else None
+        lib().orc_glwe_encrypt_cdt(self.pctx, k, p64(u64(sk_ntt)), mp, p64(u64(scale)), sigma, seed, stream0, index,
+                                   p64(ct))
+        return ct
 
     def ternary(self, seed, stream):
         out = np.zeros(self.L * self.n, np.uint64)

@@ -1568,3 +1568,63 @@ void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree
     free(tmp);
     free(perm);
 }
+
+/* ======================================================================
+ * Encryption with the CDT Gaussian sampler (reproducible on the device)
+ * ====================================================================== */
+uint32_t orc_cdt_table(double sigma, uint64_t *cdt, uint32_t cap) {
+    const uint32_t B = (uint32_t)ceil(24.0 * sigma);
+    if (B + 1 > cap) return 0;
+    double total = 0;
+    for (int64_t m = -(int64_t)B; m <= (int64_t)B; ++m) total += exp(-(double)(m * m) / (2.0 * sigma * sigma));
+    double acc = 0;
+    for (uint32_t m = 0; m <= B; ++m) {
+        const double rho = exp(-(double)m * m / (2.0 * sigma * sigma));
+        acc += (m == 0 ? rho : 2.0 * rho) / total;
+        double v = acc * 9223372036854775808.0; /* 2^63 */
+        cdt[m] = v >= 9223372036854775808.0 ? (1ull << 63) : (uint64_t)v;
+    }
+    cdt[B] = 1ull << 63;
+    return B + 1;
+}
+
+int64_t orc_cdt_sample(const uint64_t *cdt, uint32_t entries, uint64_t seed, uint64_t stream, uint64_t x) {
+    const uint64_t u = orc_hash64(seed, stream, x, 0);
+    const uint64_t v = u >> 1;
+    uint32_t lo = 0, hi = entries - 1; /* least m with v < cdt[m]; cdt[entries-1] = 2^63 > v */
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (v < cdt[mid]) hi = mid; else lo = mid + 1;
+    }
+    return (lo > 0 && (u & 1)) ? -(int64_t)lo : (int64_t)lo;
+}
+
+void orc_glwe_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *sk_ntt, const uint64_t *msg,
+                          const uint64_t *scale, double sigma, uint64_t seed, uint64_t stream0, uint64_t index,
+                          uint64_t *ct) {
+    const size_t n = c->n;
+    const uint32_t L = c->L;
+    const size_t poly = (size_t)L * n;
+    uint64_t cdt[512];
+    const uint32_t entries = orc_cdt_table(sigma, cdt, 512);
+    uint64_t *b = ct + (size_t)k * poly;
+    for (size_t x = 0; x < n; ++x) {
+        const int64_t e = orc_cdt_sample(cdt, entries, seed, stream0 + (1ull << 32) + index, x);
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint64_t q = c->tables[l]->q;
+            b[(size_t)l * n + x] = e >= 0 ? (uint64_t)e % q : q - (uint64_t)(-e) % q;
+        }
+    }
+    for (uint32_t l = 0; l < L; ++l) {
+        if (msg) orc_add_mul_scalar_assign(b + (size_t)l * n, msg + (size_t)l * n, scale[l], n, c->tables[l]->q);
+        orc_ntt_forward(c->tables[l], b + (size_t)l * n);
+    }
+    for (uint32_t i = 0; i < k; ++i) {
+        uint64_t *a = ct + (size_t)i * poly;
+        for (uint32_t l = 0; l < L; ++l)
+            orc_fill_uniform(seed, stream0 + (index * k + i) * L + l, c->tables[l]->q, n, a + (size_t)l * n);
+        for (uint32_t l = 0; l < L; ++l)
+            orc_add_mul_assign(b + (size_t)l * n, a + (size_t)l * n, sk_ntt + i * poly + (size_t)l * n, n,
+                               c->tables[l]->q);
+    }
+}

@@ -295,6 +295,21 @@ void orc_ntt_auto_perm(uint32_t log_n, uint64_t degree, uint32_t *perm);
 void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree, const uint64_t *key,
                            const uint64_t *ct_in, uint64_t *ct_out);
 
+/* ---- encryption with the device-reproducible sampler (CDT Gaussian) ----
+ * Discrete Gaussian over [-B, B], B = ceil(24 sigma) (the reference's bound,
+ * primus_distr/src/common.rs:282): cdt[m] = floor(2^63 * P(|e| <= m)) for
+ * m = 0..B (cdt[B] = 2^63); u = hash64(seed, stream, x, 0): |e| = the least m
+ * with (u >> 1) < cdt[m], negative when m > 0 and u & 1.  Returns B + 1. */
+uint32_t orc_cdt_table(double sigma, uint64_t *cdt, uint32_t cap);
+int64_t orc_cdt_sample(const uint64_t *cdt, uint32_t entries, uint64_t seed, uint64_t stream, uint64_t x);
+/* secret-key GLWE encryption (DcrtGlweSecretKey::encrypt_inplace, secret_key/glwe.rs:386-424)
+ * of ciphertext `index` of a batch: a_i limb l uniform with stream
+ * stream0 + (index k + i) L + l; e with stream stream0 + 2^32 + index;
+ * b = NTT(e + scale_l msg) + sum a_i s_i (msg coefficient form [L][N] or NULL) */
+void orc_glwe_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *sk_ntt, const uint64_t *msg,
+                          const uint64_t *scale, double sigma, uint64_t seed, uint64_t stream0, uint64_t index,
+                          uint64_t *ct);
+
 /* ---- HEXL-style AVX-512 IFMA52 transforms (hexl_ifma.c): the reference's fastest
  * CPU path, timed as the CPU baseline (q < 2^50, n >= 16, host with avx512ifma) */
 typedef struct orc_hexl_table orc_hexl_table;

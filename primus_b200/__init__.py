@@ -7,7 +7,7 @@ trait API.  Importing it loads the library and fails loudly when it is absent.
 from ._native import (DeviceBuffer, Event, PrimusGpuError, Stream, device_count, launch_count,  # noqa: F401
                       synchronize)
 from .lattice import (BaseConverter, GadgetBasis, RnsBase, RnsError, external_product,  # noqa: F401
-                      external_product_coeff, HybridKeySwitch, glwe_automorphism, BfvDecryptor,
+                      external_product_coeff, HybridKeySwitch, glwe_automorphism, BfvDecryptor, GlweEncryptor,
                       ext_product_workspace_size, glev_mac_big_uint_poly, glev_mac_crt_poly, key_switch,
                       key_switch_workspace_size)
 from .server import (Request, Server, ext_product_request, key_switch_request,  # noqa: F401

@@ -237,3 +237,31 @@ class BfvDecryptor:
             self.close()
         except Exception:
             pass
+
+
+class GlweEncryptor:
+    """Secret-key GLWE encryption on the device with reproducible samplers
+    (pg_glwe_encryptor_* / pg_glwe_encrypt)."""
+
+    def __init__(self, table, sigma: float = 3.2):
+        h = C.c_void_p()
+        call("pg_glwe_encryptor_create", table.h, float(sigma), C.byref(h))
+        self.h = h.value
+        self.table, self.sigma = table, sigma
+
+    def encrypt(self, k: int, sk_ntt: DeviceBuffer, msg: DeviceBuffer | None, scale, seed: int, stream0: int,
+                ct: DeviceBuffer, batch: int, stream=None):
+        sc = np.ascontiguousarray(np.asarray(scale if scale is not None else [0] * self.table.L, dtype=np.uint64))
+        call("pg_glwe_encrypt", self.h, k, sk_ntt.ptr, msg.ptr if msg is not None else None, ptr(sc), seed, stream0,
+             ct.ptr, batch, _sh(stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().pg_glwe_encryptor_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
