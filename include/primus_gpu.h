@@ -63,6 +63,14 @@ int pg_host_alloc(void **h_ptr, size_t bytes); /* page-locked */
 int pg_host_free(void *h_ptr);
 int pg_memcpy_h2d(void *d_dst, const void *h_src, size_t bytes, void *stream);
 int pg_memcpy_d2h(void *h_dst, const void *d_src, size_t bytes, void *stream);
+/* Wire / disk format of every container (GLWE, GLev, GGSW, keys, DCRT polys):
+ * the little-endian u64 words back to back, the reference's bytemuck cast
+ * (primus_lattice/src/macros/mod.rs:39-97 from_bytes_assign / to_bytes_inplace).
+ * A byte count other than 8 x words is refused (the reference panics).  On
+ * little-endian hosts the bytes are the words' memory image, so these are
+ * checked synchronous copies into / out of a device buffer. */
+int pg_from_bytes(uint64_t *d_dst, size_t words, const uint8_t *h_bytes, size_t nbytes);
+int pg_to_bytes(const uint64_t *d_src, size_t words, uint8_t *h_bytes, size_t nbytes);
 int pg_memcpy_d2d(void *d_dst, const void *d_src, size_t bytes, void *stream);
 int pg_memset(void *d_ptr, int value, size_t bytes, void *stream);
 int pg_stream_create(void **stream);

@@ -185,6 +185,20 @@ class DeviceBuffer:
         call("pg_stream_synchronize", _sh(stream))
         return out.reshape(shape) if shape is not None else out
 
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "DeviceBuffer":
+        """The reference's from_bytes: little-endian u64 words (len(data) must be a multiple of 8)."""
+        b = cls(len(data) // 8)
+        buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        call("pg_from_bytes", b.ptr, b.count, buf, len(data))
+        return b
+
+    def to_bytes(self) -> bytes:
+        """The reference's to_bytes: the words as little-endian bytes."""
+        buf = (C.c_uint8 * (self.count * 8))()
+        call("pg_to_bytes", self.ptr, self.count, buf, self.count * 8)
+        return bytes(buf)
+
     def zero(self, stream=None):
         call("pg_memset", self.ptr, 0, self.count * 8, _sh(stream))
 

@@ -341,6 +341,24 @@ int pg_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, void* stream) {
     return PG_OK;
 }
 
+int pg_from_bytes(uint64_t* d_dst, size_t words, const uint8_t* h_bytes, size_t nbytes) {
+    if (nbytes != words * sizeof(uint64_t))
+        return set_error(PG_ERR_INVALID_ARGUMENT, "byte count is not 8 x the destination's word count");
+    if (nbytes == 0) return PG_OK;
+    if (!d_dst || !h_bytes) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PG_CUDA(cudaMemcpy(d_dst, h_bytes, nbytes, cudaMemcpyHostToDevice));
+    return PG_OK;
+}
+
+int pg_to_bytes(const uint64_t* d_src, size_t words, uint8_t* h_bytes, size_t nbytes) {
+    if (nbytes != words * sizeof(uint64_t))
+        return set_error(PG_ERR_INVALID_ARGUMENT, "byte count is not 8 x the source's word count");
+    if (nbytes == 0) return PG_OK;
+    if (!d_src || !h_bytes) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PG_CUDA(cudaMemcpy(h_bytes, d_src, nbytes, cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
 int pg_memcpy_d2d(void* d_dst, const void* d_src, size_t bytes, void* stream) {
     if (bytes == 0) return PG_OK;
     PG_CUDA(cudaMemcpyAsync(d_dst, d_src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));

@@ -54,3 +54,16 @@ def test_device_encrypt_decrypt_round_trip(gpu):
     out = gpu.DeviceBuffer(batch * n)
     dec.decrypt(k, dsk, ct, out, batch)
     assert np.array_equal(out.numpy().reshape(batch, n), msg)
+
+
+def test_wire_format_round_trip(gpu):
+    # primus_lattice/src/macros/mod.rs:39-97: containers travel as little-endian u64 bytes
+    from primus_b200 import _native as nat
+    import ctypes as C
+    x = O.uniform(3, 4, (1 << 50) - 27, 4096)
+    d = gpu.DeviceBuffer.from_bytes(x.astype("<u8").tobytes())
+    assert np.array_equal(d.numpy(), x)
+    assert d.to_bytes() == x.astype("<u8").tobytes()
+    bad = (C.c_uint8 * 15)()
+    assert nat.lib().pg_from_bytes(d.ptr, d.count, bad, 15) == nat.PG_ERR_INVALID_ARGUMENT
+    assert nat.lib().pg_to_bytes(d.ptr, d.count, bad, 15) == nat.PG_ERR_INVALID_ARGUMENT
