@@ -338,6 +338,7 @@ def run_gpu(args):
                          "uneven_batch": bench_uneven(P, stream),
                          "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu),
                          "hybrid_ks": bench_hybrid_ks(P, stream),
+                         "widened": bench_widened(P, stream),
                          "served_mixed": bench_served(P, stream),
                          "autotune_L24": bench_autotune(P)}
         out = {
@@ -508,6 +509,45 @@ def bench_hybrid_ks(P, stream, batches=(1, 8, 32)):
     return res
 
 
+def bench_widened(P, stream, batch=64):
+    """The rows built beside the hot path, on the key-switch shape (N = 2^15,
+    L = 16 primes < 2^50, k = 1): GLWE encryption, BFV decryption and the
+    NTT-domain automorphism (BigUint gadget, log_basis 50 -> 16 digits), per
+    ciphertext, with the HBM bytes each one must move."""
+    import numpy as np
+    log_n, L, k, n = 15, 16, 1, 1 << 15
+    moduli = P.ntt_primes(1 << 50, 2 * n, L)
+    tab = P.DcrtTable(log_n, moduli)
+    tab.autotune(16)
+    ct_words = (k + 1) * L * n
+    sk = P.DeviceBuffer(k * L * n)
+    tab.fill_uniform(sk, k, seed=0x51, stream=stream)
+    msg = P.DeviceBuffer(batch * L * n)
+    tab.fill_uniform(msg, batch, seed=0x52, stream=stream)
+    ct = P.DeviceBuffer(batch * ct_words)
+    out = P.DeviceBuffer(batch * ct_words)
+    enc = P.GlweEncryptor(tab)
+    scale = [1] * L
+    res = {"shape": "N=2^15, L=16 primes < 2^50, k=1, batch %d" % batch}
+    ms = _time_stream(P, stream, lambda: enc.encrypt(k, sk, msg, scale, 7, 0, ct, batch, stream=stream), 5)
+    nbytes = batch * (ct_words + L * n) * 8
+    res["encrypt"] = {"us_per_ciphertext": ms * 1e3 / batch, "hbm_gbs": nbytes / (ms / 1e3) / 1e9}
+    dec = P.BfvDecryptor(tab, 65537, 2199023190017)
+    m = P.DeviceBuffer(batch * n)
+    ms = _time_stream(P, stream, lambda: dec.decrypt(k, sk, ct, m, batch, stream=stream), 5)
+    nbytes = batch * (ct_words + n) * 8
+    res["decrypt"] = {"us_per_ciphertext": ms * 1e3 / batch, "hbm_gbs": nbytes / (ms / 1e3) / 1e9}
+    g = P.GadgetBasis(P.RnsBase(moduli), 50)
+    key = P.DeviceBuffer(k * g.d * (k + 1) * L * n)
+    tab.fill_uniform(key, k * g.d * (k + 1), seed=0x53, stream=stream)
+    ws = P.DeviceBuffer(P.lattice.nat.lib().pg_glwe_automorphism_workspace_size(tab.h, g.h, k, batch) // 8 + 1)
+    ms = _time_stream(P, stream, lambda: P.glwe_automorphism(tab, g, k, 5, key, ct, out, batch, workspace=ws,
+                                                             stream=stream), 3)
+    res["automorphism"] = {"us_per_ciphertext": ms * 1e3 / batch, "digits": g.d,
+                           "rows_transformed_per_ciphertext": L + g.d * L}
+    return res
+
+
 def run_workload(args):
     """One secondary workload alone (for profiler captures and focused runs)."""
     import primus_b200 as P
@@ -516,6 +556,7 @@ def run_workload(args):
           "uneven_batch": lambda: bench_uneven(P, stream),
           "ext_product": lambda: bench_ext_product(P, stream, cpu=not args.no_cpu),
           "hybrid_ks": lambda: bench_hybrid_ks(P, stream),
+          "widened": lambda: bench_widened(P, stream),
           "served_mixed": lambda: bench_served(P, stream),
           "autotune_L24": lambda: bench_autotune(P)}[args.workload]
     print(json.dumps({"workload_name": args.workload, **fn()}))
@@ -680,8 +721,8 @@ def main(argv=None):
     ap.add_argument("--polys", type=int, default=POLYS,
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")
     ap.add_argument("--workload", default=None,
-                    choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "served_mixed",
-                             "autotune_L24"],
+                    choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "widened",
+                             "served_mixed", "autotune_L24"],
                     help="run only this secondary workload and print its result")
     args = ap.parse_args(argv)
     set_polys(args.polys)
