@@ -128,8 +128,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
-    """One process per GPU under torchrun; returns (rank, world, local_rank, dist-or-None)."""
+def dist_setup(n_gpus, backend="nccl"):
+    """One process per GPU under torchrun; returns (rank, world, local_rank, dist-or-None).
+    The path runs as replicas: the process group carries only the barriers and the
+    max-over-ranks of the timings (gloo for the CPU tests of that logic)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -138,9 +140,12 @@ def dist_setup(n_gpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
         return rank, world, local, dist
     return rank, world, local, None
 
@@ -149,7 +154,8 @@ def dist_max(dist, value: float, local: int) -> float:
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -202,7 +208,9 @@ def cpu_reference(moduli, seconds_target=12.0, threads=None, path=None):
 
 
 def run_reference(args):
-    rank, world, local, dist = dist_setup(args.gpus)
+    # a CPU arm: under torchrun rank 0 alone times it and prints; the other ranks
+    # exit without work (no process group, so nothing waits on them)
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle as O

@@ -197,13 +197,6 @@ __global__ void __launch_bounds__(256) finish_kernel(FinishArgs a) {
     }
 }
 
-// grid for a kernel whose x dimension covers `inner` elements with 256 threads
-// and whose y dimension covers `outer` rows (both loop when capped)
-dim3 grid2(size_t inner, size_t outer) {
-    const size_t bx = std::min<size_t>((inner + 255) / 256, 4096);
-    const size_t by = std::min<size_t>(outer, 65535);
-    return dim3((unsigned)std::max<size_t>(bx, 1), (unsigned)std::max<size_t>(by, 1));
-}
 
 
 // a table view over limbs [first, first + count) of t (device arrays shared)

@@ -20,6 +20,23 @@ void clear_error();
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// ---- launch geometry for elementwise kernels
+// 1D grid-stride launch: enough CTAs of `threads` for `work` items, at most 2048
+// resident threads' worth per SM (148 SMs)
+inline unsigned grid_for(size_t work, unsigned threads) {
+    const size_t cap = 148ull * 2048 / threads;
+    const size_t b = (work + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : (b < cap ? b : cap));
+}
+// 2D launch: x covers `inner` elements with 256 threads per CTA, y covers
+// `outer` rows (polys, ciphertexts); both loop inside the kernel when capped
+inline dim3 grid2(size_t inner, size_t outer) {
+    size_t bx = (inner + 255) / 256, by = outer;
+    bx = bx < 1 ? 1 : (bx > 4096 ? 4096 : bx);
+    by = by < 1 ? 1 : (by > 65535 ? 65535 : by);
+    return dim3((unsigned)bx, (unsigned)by);
+}
+
 // ---- scratch: stream-ordered allocations from a library-owned pool per device
 // that keeps freed memory (release threshold = unlimited), so a call that needs
 // scratch does not map fresh memory after every synchronize

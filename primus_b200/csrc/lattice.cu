@@ -173,19 +173,7 @@ __global__ void __launch_bounds__(256) auto_perm_kernel(const uint64_t* __restri
     }
 }
 
-unsigned grid_for(size_t work, unsigned threads) {
-    const size_t cap = 148ull * 2048 / threads;
-    size_t b = (work + threads - 1) / threads;
-    return (unsigned)std::max<size_t>(1, std::min(b, cap));
-}
 
-// grid for a kernel whose x dimension covers `inner` elements with 256 threads
-// and whose y dimension covers `outer` rows (both loop when capped)
-dim3 grid2(size_t inner, size_t outer) {
-    const size_t bx = std::min<size_t>((inner + 255) / 256, 4096);
-    const size_t by = std::min<size_t>(outer, 65535);
-    return dim3((unsigned)std::max<size_t>(bx, 1), (unsigned)std::max<size_t>(by, 1));
-}
 
 int check_compat(const pg_ntt_table* t, const pg_gadget_basis* g) {
     if (!t || !g) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL table or basis");

@@ -128,12 +128,6 @@ __global__ void __launch_bounds__(256) fill_uniform_kernel(uint64_t* out, const 
     }
 }
 
-// x over the elements of one poly (256 threads per CTA), y over polys
-static dim3 grid2(uint64_t inner, uint64_t polys) {
-    const uint64_t bx = std::min<uint64_t>((inner + 255) / 256, 4096);
-    const uint64_t by = std::min<uint64_t>(polys, 65535);
-    return dim3((unsigned)std::max<uint64_t>(bx, 1), (unsigned)std::max<uint64_t>(by, 1));
-}
 
 
 template <int OP>

@@ -358,12 +358,6 @@ __global__ void __launch_bounds__(128) gadget_kernel(GadgetArgs a) {
     }
 }
 
-unsigned grid_for(size_t work, unsigned threads) {
-    const size_t cap = 148ull * 2048 / threads;
-    size_t b = (work + threads - 1) / threads;
-    return (unsigned)std::max<size_t>(1, std::min(b, cap));
-}
-
 void free_base(pg_rns_base* b) {
     if (!b) return;
     cudaFree(b->d_moduli);
