@@ -8,9 +8,11 @@
 // budget, so admission is by memory -- a batch takes as many pending requests
 // of one kind and shape as fit in its slot's scratch.  Requests that arrive
 // while other batches are on the GPU wait for the next free slot, and batches
-// on different slots overlap on the device.  Completion is signalled from the
-// stream by a host callback (no device-side waiting), which frees the slot,
-// timestamps each request and wakes the worker and any waiting clients.
+// on different slots overlap on the device.  Completion is an event recorded
+// after each batch's last launch and polled by a completion thread (no
+// device-side waiting), which frees the slot, timestamps each request and wakes
+// the worker and any waiting clients.  The idle worker spins briefly before it
+// sleeps, so a request arriving right after a batch is not delayed by a wake-up.
 //
 // Batches reuse the library's batched paths: pg_polymul_batch (descriptor
 // driven NTT launches), and for external products / key switches a gather of
@@ -86,7 +88,9 @@ struct Slot {
     uint64_t** d_ptrs = nullptr;
     size_t ptr_cap = 0;
     pg_polymul_batch* polymul = nullptr;
+    cudaEvent_t done_ev = nullptr;  // recorded after the batch's last launch
     bool busy = false;
+    bool in_flight = false;  // on the GPU, watched by the completion thread
     std::vector<uint64_t> tickets;  // requests of the batch in flight
     int status = PG_OK;
 };
@@ -98,10 +102,11 @@ struct pg_server {
     std::vector<Key> keys;
     std::vector<Slot> slots;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_poll;
+    std::atomic<int> pending_n{0}, free_n{0};  // mirrors of pending.size() and idle slots (written under mu)
     std::deque<Req> pending;
     std::vector<TicketState*> tickets;  // index = ticket
-    std::thread worker;
+    std::thread worker, poller;
     bool stop = false;
     int device = 0;
     // statistics
@@ -113,8 +118,8 @@ struct pg_server {
 
 namespace {
 
-void CUDART_CB on_batch_done(void* arg) {
-    Slot* s = (Slot*)arg;
+// completes the batch of slot s: timestamps its requests and frees the slot
+void on_batch_done(Slot* s) {
     pg_server* srv = s->server;
     const double t = now_us();
     {
@@ -129,9 +134,47 @@ void CUDART_CB on_batch_done(void* arg) {
         }
         s->tickets.clear();
         s->busy = false;
+        s->in_flight = false;
+        srv->free_n.fetch_add(1);
     }
     srv->cv_done.notify_all();
     srv->cv_work.notify_all();
+}
+
+// Completion thread: polls the events of the batches on the GPU (no device-side
+// waiting, no driver callback thread in the path), so a finished batch frees
+// its slot a few microseconds after its last kernel.
+void poller_loop(pg_server* srv) {
+    cudaSetDevice(srv->device);
+    std::vector<Slot*> watch;
+    std::unique_lock<std::mutex> lock(srv->mu);
+    for (;;) {
+        srv->cv_poll.wait(lock, [&] {
+            if (srv->stop) return true;
+            for (auto& s : srv->slots)
+                if (s.in_flight) return true;
+            return false;
+        });
+        if (srv->stop) return;
+        watch.clear();
+        for (auto& s : srv->slots)
+            if (s.in_flight) watch.push_back(&s);
+        lock.unlock();
+        bool any = false;
+        for (Slot* s : watch) {
+            const cudaError_t e = cudaEventQuery(s->done_ev);
+            if (e == cudaErrorNotReady) continue;
+            if (e != cudaSuccess) {
+                s->status = cuda_status(e, "server batch");
+                std::lock_guard<std::mutex> g(srv->mu);
+                srv->worker_error = pg_last_error();
+            }
+            on_batch_done(s);
+            any = true;
+        }
+        if (!any) std::this_thread::yield();
+        lock.lock();
+    }
 }
 
 size_t request_scratch(const pg_server* srv, const pg_request& r) {
@@ -212,6 +255,15 @@ void worker_loop(pg_server* srv) {
     std::unique_lock<std::mutex> lock(srv->mu);
     for (;;) {
         Slot* slot = nullptr;
+        if (!srv->stop && (srv->pending.empty() || srv->free_n.load() == 0)) {
+            // idle: spin briefly on the lock-free mirrors before sleeping, so a
+            // request arriving right after a batch does not pay a thread wake-up
+            lock.unlock();
+            const double t0 = now_us();
+            while (now_us() - t0 < 100.0 && (srv->pending_n.load() == 0 || srv->free_n.load() == 0))
+                std::this_thread::yield();
+            lock.lock();
+        }
         srv->cv_work.wait(lock, [&] {
             if (srv->stop) return true;
             if (srv->pending.empty()) return false;
@@ -235,6 +287,7 @@ void worker_loop(pg_server* srv) {
                     used += need;
                     batch.push_back(*it);
                     it = srv->pending.erase(it);
+                    srv->pending_n.fetch_sub(1);
                     continue;
                 }
                 if (need > slot->scratch_bytes) {  // cannot ever fit (checked at submit)
@@ -247,6 +300,7 @@ void worker_loop(pg_server* srv) {
         }
         if (batch.empty()) continue;
         slot->busy = true;
+        srv->free_n.fetch_sub(1);
         slot->tickets.clear();
         for (auto& b : batch) slot->tickets.push_back(b.ticket);
         ++srv->batches;
@@ -256,10 +310,17 @@ void worker_loop(pg_server* srv) {
         int rc = run_batch(srv, *slot, batch);
         slot->status = rc;
         if (rc == PG_OK) {
-            cudaError_t e = cudaLaunchHostFunc(slot->stream, on_batch_done, slot);
-            if (e != cudaSuccess) rc = cuda_status(e, "cudaLaunchHostFunc");
+            cudaError_t e = cudaEventRecord(slot->done_ev, slot->stream);
+            if (e != cudaSuccess) rc = cuda_status(e, "server: completion event");
         }
         const double enq = now_us() - t_enq;
+        if (rc == PG_OK) {
+            {
+                std::lock_guard<std::mutex> g(srv->mu);
+                slot->in_flight = true;
+            }
+            srv->cv_poll.notify_one();
+        }
         if (rc != PG_OK) {
             // the batch never reached the GPU: fail its requests now
             slot->status = rc;
@@ -299,6 +360,7 @@ int pg_server_create(const pg_server_config* cfg, const pg_ntt_table* const* pol
         s.server = srv;
         s.index = (int)i;
         cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done_ev, cudaEventDisableTiming);
         if (e == cudaSuccess && share) e = cudaMalloc(&s.scratch, share);
         if (e != cudaSuccess) {
             pg_server_destroy(srv);
@@ -320,7 +382,9 @@ int pg_server_create(const pg_server_config* cfg, const pg_ntt_table* const* pol
         }
     }
     srv->tickets.reserve(1 << 16);
+    srv->free_n.store((int)srv->slots.size());
     srv->worker = std::thread(worker_loop, srv);
+    srv->poller = std::thread(poller_loop, srv);
     *out = srv;
     return PG_OK;
 }
@@ -332,11 +396,14 @@ int pg_server_destroy(pg_server* srv) {
         srv->stop = true;
     }
     srv->cv_work.notify_all();
+    srv->cv_poll.notify_all();
     if (srv->worker.joinable()) srv->worker.join();
+    if (srv->poller.joinable()) srv->poller.join();
     for (auto& s : srv->slots) {
         if (s.stream) cudaStreamSynchronize(s.stream);
         pg_polymul_batch_destroy(s.polymul);
         if (s.stream) cudaStreamDestroy(s.stream);
+        if (s.done_ev) cudaEventDestroy(s.done_ev);
         cudaFree(s.scratch);
         cudaFreeHost(s.h_ptrs);
         cudaFree(s.d_ptrs);
@@ -416,6 +483,7 @@ int pg_server_submit(pg_server* srv, const pg_request* req, uint64_t* ticket) {
     ts->t_submit = now_us();
     srv->tickets.push_back(ts);
     srv->pending.push_back(Req{*req, tk, ts->t_submit});
+    srv->pending_n.fetch_add(1);
     ++srv->submitted;
     *ticket = tk;
     lock.unlock();
