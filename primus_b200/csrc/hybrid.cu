@@ -89,35 +89,51 @@ __global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
         const uint32_t lo = g * a.alpha, hi = min(a.L, lo + a.alpha), ag = hi - lo;
         const ulonglong2* mat = a.gmat + a.gmat_off[g];
         const uint32_t* outl = a.gout + a.gout_off[g];
-        for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.N; x += gridDim.x * blockDim.x) {
-            const uint64_t* src = src0 + x;
-            uint64_t* dst = dst0 + x;
-            uint64_t tv[AMAX];
+        // two coefficients per thread (x and x + blockDim.x): twice the independent
+        // work per loaded matrix entry
+        for (uint32_t x0 = blockIdx.x * 2 * blockDim.x + threadIdx.x; x0 < a.N; x0 += gridDim.x * 2 * blockDim.x) {
+            const uint32_t x1 = x0 + blockDim.x;
+            const bool two = x1 < a.N;
+            uint64_t tv0[AMAX], tv1[AMAX];
 #pragma unroll
             for (uint32_t m = 0; m < AMAX; ++m) {
-                tv[m] = 0;
+                tv0[m] = tv1[m] = 0;
                 if (m < ag) {
                     const uint32_t l = lo + m;
-                    const uint64_t v = src[(size_t)l * a.N];
-                    dst[(size_t)l * a.N] = v;
                     const ulonglong2 f = a.ginv[l];
-                    tv[m] = shoup_mul(f.x, f.y, v, a.moduli[l]);
+                    const uint64_t ql = a.moduli[l];
+                    const uint64_t v0 = src0[(size_t)l * a.N + x0];
+                    dst0[(size_t)l * a.N + x0] = v0;
+                    tv0[m] = shoup_mul(f.x, f.y, v0, ql);
+                    if (two) {
+                        const uint64_t v1 = src0[(size_t)l * a.N + x1];
+                        dst0[(size_t)l * a.N + x1] = v1;
+                        tv1[m] = shoup_mul(f.x, f.y, v1, ql);
+                    }
                 }
             }
+#pragma unroll 2
             for (uint32_t j = 0; j < LK - ag; ++j) {
                 const uint32_t r = outl[j];
-                const uint64_t rq = a.moduli[r];
-                uint64_t y = 0;  // sum of at most 8 lazy products in [0, 2 r): below 16 r < 2^64
+                const uint64_t rq = a.moduli[r], nq = 0 - rq;
+                // sums of at most 8 lazy products in [0, 2 r): below 16 r < 2^64
+                uint64_t y0 = 0, y1 = 0;
 #pragma unroll
                 for (uint32_t m = 0; m < AMAX; ++m)
                     if (m < ag) {
                         const ulonglong2 w = mat[j * ag + m];
-                        y += shoup_lazy(w.x, w.y, tv[m], rq);
+                        y0 += shoup_lazy_nq(w.x, w.y, tv0[m], nq);
+                        y1 += shoup_lazy_nq(w.x, w.y, tv1[m], nq);
                     }
                 // [0, 4 r) is enough: the forward NTT that follows accepts inputs below
                 // 4q and returns canonical values of the same residues
-                if (AMAX > 4) y = y >= 8 * rq ? y - 8 * rq : y;
-                dst[(size_t)r * a.N] = y >= 4 * rq ? y - 4 * rq : y;
+                if (AMAX > 4) {
+                    y0 = y0 >= 8 * rq ? y0 - 8 * rq : y0;
+                    y1 = y1 >= 8 * rq ? y1 - 8 * rq : y1;
+                }
+                uint64_t* d = dst0 + (size_t)r * a.N;
+                d[x0] = y0 >= 4 * rq ? y0 - 4 * rq : y0;
+                if (two) d[x1] = y1 >= 4 * rq ? y1 - 4 * rq : y1;
             }
         }
     }
@@ -139,27 +155,37 @@ struct PConvArgs {
 template <uint32_t KMAX>
 __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
     for (size_t p = blockIdx.y; p < a.pc; p += gridDim.y) {
-        for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < a.N; x += gridDim.x * blockDim.x) {
-            uint64_t tv[KMAX];
+        const uint64_t* src = a.accp + (p * a.K) * a.N;
+        uint64_t* dst = a.conv + (p * a.L) * a.N;
+        // two coefficients per thread (x and x + blockDim.x)
+        for (uint32_t x0 = blockIdx.x * 2 * blockDim.x + threadIdx.x; x0 < a.N; x0 += gridDim.x * 2 * blockDim.x) {
+            const uint32_t x1 = x0 + blockDim.x;
+            const bool two = x1 < a.N;
+            uint64_t tv0[KMAX], tv1[KMAX];
 #pragma unroll
             for (uint32_t k = 0; k < KMAX; ++k) {
-                tv[k] = 0;
+                tv0[k] = tv1[k] = 0;
                 if (k < a.K) {
                     const ulonglong2 f = a.pinv_k[k];
-                    tv[k] = shoup_mul(f.x, f.y, a.accp[(p * a.K + k) * a.N + x], a.moduli[a.L + k]);
+                    const uint64_t pk = a.moduli[a.L + k];
+                    tv0[k] = shoup_mul(f.x, f.y, src[(size_t)k * a.N + x0], pk);
+                    if (two) tv1[k] = shoup_mul(f.x, f.y, src[(size_t)k * a.N + x1], pk);
                 }
             }
-            uint64_t* dst = a.conv + (p * a.L) * a.N + x;
+#pragma unroll 2
             for (uint32_t l = 0; l < a.L; ++l) {
-                const uint64_t ql = a.moduli[l];
-                uint64_t y = 0;  // sum of at most 8 lazy products in [0, 2 q_l): below 16 q_l < 2^64
+                const uint64_t ql = a.moduli[l], nq = 0 - ql;
+                // sums of at most 8 lazy products in [0, 2 q_l): below 16 q_l < 2^64
+                uint64_t y0 = 0, y1 = 0;
 #pragma unroll
                 for (uint32_t k = 0; k < KMAX; ++k)
                     if (k < a.K) {
                         const ulonglong2 w = a.pmat[l * a.K + k];
-                        y += shoup_lazy(w.x, w.y, tv[k], ql);
+                        y0 += shoup_lazy_nq(w.x, w.y, tv0[k], nq);
+                        y1 += shoup_lazy_nq(w.x, w.y, tv1[k], nq);
                     }
-                dst[(size_t)l * a.N] = reduce_below_16q(y, ql);
+                dst[(size_t)l * a.N + x0] = reduce_below_16q(y0, ql);
+                if (two) dst[(size_t)l * a.N + x1] = reduce_below_16q(y1, ql);
             }
         }
     }
@@ -392,9 +418,9 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     ma.dnum = h->dnum;
     ma.log_n = t->log_n;
     if (h->alpha <= 4)
-        modup_kernel<4><<<grid2(n, ma.polys * h->dnum), 256, 0, st>>>(ma);
+        modup_kernel<4><<<grid2((n + 1) / 2, ma.polys * h->dnum), 256, 0, st>>>(ma);
     else
-        modup_kernel<kMaxAlpha><<<grid2(n, ma.polys * h->dnum), 256, 0, st>>>(ma);
+        modup_kernel<kMaxAlpha><<<grid2((n + 1) / 2, ma.polys * h->dnum), 256, 0, st>>>(ma);
     count_launch();
     PG_LAUNCH_CHECK("modup_kernel launch");
     int rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
@@ -419,9 +445,9 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     pa.K = h->K;
     pa.log_n = t->log_n;
     if (h->K <= 4)
-        pconv_kernel<4><<<grid2(n, pa.pc), 256, 0, st>>>(pa);
+        pconv_kernel<4><<<grid2((n + 1) / 2, pa.pc), 256, 0, st>>>(pa);
     else
-        pconv_kernel<kMaxK><<<grid2(n, pa.pc), 256, 0, st>>>(pa);
+        pconv_kernel<kMaxK><<<grid2((n + 1) / 2, pa.pc), 256, 0, st>>>(pa);
     count_launch();
     PG_LAUNCH_CHECK("pconv_kernel launch");
     rc = launch_ntt(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, MODE_FWD, st);
