@@ -55,6 +55,41 @@ PG_DEV uint64_t shoup_lazy_nq(uint64_t w, uint64_t wq, uint64_t b, uint64_t nq) 
     return r;
 }
 
+// The same product with the quotient estimate formed without the high word of
+// the low 32x32 partial product (one multiply fewer): the estimate is the exact
+// Shoup quotient or one less, so the result lies in [0, 3q).  Used only inside
+// transforms whose outputs are reduced to canonical values at the end.
+PG_DEV uint64_t shoup_lazy3_nq(uint64_t w, uint64_t wq, uint64_t b, uint64_t nq) {
+    uint64_t r;
+    asm("{\n\t"
+        ".reg .u32 a0, a1, b0, b1, m0, m1, s0, s1, c2, w0, w1, n0, n1, h0, h1, r0, r1;\n\t"
+        ".reg .u64 m, hw, acc;\n\t"
+        "mov.b64 {a0, a1}, %2;\n\t"
+        "mov.b64 {b0, b1}, %3;\n\t"
+        "mul.wide.u32 m, a0, b1;\n\t"
+        "mov.b64 {m0, m1}, m;\n\t"
+        "mad.lo.cc.u32 s0, a1, b0, m0;\n\t"
+        "madc.hi.cc.u32 s1, a1, b0, m1;\n\t"
+        "addc.u32 c2, 0, 0;\n\t"
+        "mov.b64 m, {s1, c2};\n\t"
+        "mad.wide.u32 hw, a1, b1, m;\n\t"
+        "mov.b64 {h0, h1}, hw;\n\t"
+        "mov.b64 {w0, w1}, %1;\n\t"
+        "mov.b64 {n0, n1}, %4;\n\t"
+        "mul.wide.u32 acc, w0, b0;\n\t"
+        "mad.wide.u32 acc, n0, h0, acc;\n\t"
+        "mov.b64 {r0, r1}, acc;\n\t"
+        "mad.lo.u32 r1, w0, b1, r1;\n\t"
+        "mad.lo.u32 r1, w1, b0, r1;\n\t"
+        "mad.lo.u32 r1, n0, h1, r1;\n\t"
+        "mad.lo.u32 r1, n1, h0, r1;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(w), "l"(wq), "l"(b), "l"(nq));
+    return r;
+}
+
 PG_DEV uint64_t shoup_lazy(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) { return shoup_lazy_nq(w, wq, b, 0 - q); }
 
 // Shoup full multiply: result in [0, q)

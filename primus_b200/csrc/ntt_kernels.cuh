@@ -69,13 +69,15 @@ PG_DEV void fwd_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, 
 // Forward butterfly without the u = x mod 2q step.  Used only where the
 // canonical result is returned (transform_slice, the fused round trip): the
 // bound grows by 2q per stage, so after log2(N) <= 16 stages from [0, 4q) the
-// values stay below 36q < 2^64 for q < 2^58, and the final canonical
-// reduction yields the same residues as the Harvey schedule.
+// values stay below 52q < 2^64 for q < 2^58 (v below 3q from the one-multiply-
+// shorter Shoup estimate, so the bound grows by 3q per stage from 4q), and the
+// final canonical reduction yields the same residues as the Harvey schedule.
 PG_DEV void fwd_bfly_fast(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, uint64_t nq) {
+    const uint64_t q3 = q2 + (q2 >> 1);
     uint64_t u = x;
-    uint64_t v = shoup_lazy_nq(w.x, w.y, y, nq);
+    uint64_t v = shoup_lazy3_nq(w.x, w.y, y, nq);
     x = u + v;
-    y = u + q2 - v;
+    y = u + q3 - v;
 }
 
 // Gentleman-Sande inverse butterfly; x, y in [0, 2q) -> [0, 2q)
@@ -88,12 +90,14 @@ PG_DEV void inv_bfly(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q2, 
 
 // Inverse butterfly without the x reduction, for inputs below `bnd` (a power-of-two
 // multiple of 2q known at compile time): x = u + v (< 2 bnd), y = w (u + bnd - v)
-// in [0, 2q).  Used only where the result is canonical (the inverse always is)
-// and every q < 2^50, so that the unreduced sums stay below 2^64 (see inv_round).
+// in [0, 3q) (one-multiply-shorter Shoup estimate; 3q is below the next stage's
+// bound 2 bnd >= 4q).  Used only where the result is canonical (the inverse
+// always is) and every q < 2^50, so that the unreduced sums stay below 2^64
+// (see inv_round).
 PG_DEV void inv_bfly_fast(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t bnd, uint64_t nq) {
     uint64_t u = x, v = y;
     x = u + v;
-    y = shoup_lazy_nq(w.x, w.y, u + bnd - v, nq);
+    y = shoup_lazy3_nq(w.x, w.y, u + bnd - v, nq);
 }
 
 // Last inverse stage fused with N^-1: x = N^-1 (u+v), y = (w N^-1)(u+bnd-v),
