@@ -111,9 +111,9 @@ PG_DEV void inv_last_bfly(uint64_t& x, uint64_t& y, const ulonglong2 s, const ul
     y = b >= q ? b - q : b;
 }
 
-// First stage at which the unreduced inverse schedule reduces its values again:
-// every round that starts at or after this stage first reduces its elements to
-// [0, q).  Before it values grow at most 2^12 q (< 2^62 for q < 2^50).
+// Stage around which the unreduced inverse schedule reduces its values once: the
+// round that contains this stage first reduces its elements to [0, q).  Before
+// it values stay below 2^9 q; after it below 2^12 q (< 2^62 for q < 2^50).
 constexpr int kFastInvReduceStage = 8;
 
 // any 64-bit v -> v mod q, using floor(2^64/q) (the high word of the Barrett ratio)
@@ -189,12 +189,13 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // which stores inv_root_powers[j + 1] at j (so paired loads are aligned).  The
 // last stage of the transform (p == LOG_N-1) is the N^-1-scaled one.
 //
-// FASTI (every q < 2^50, inputs below 2q): no per-butterfly reduction of x.  A
-// round that starts before kFastInvReduceStage sees inputs below 2^p * 2q at
-// stage p; a round that starts at or after it first reduces its elements to
-// [0, q) (inv64 = floor(2^64/q)), after which stage p sees inputs below
-// 2^(p - P_LO) * 2q.  Outputs are canonical either way, so the values equal the
-// exact Harvey schedule's.
+// FASTI (every q < 2^50, inputs below 2q): no per-butterfly reduction of x.
+// Rounds before the one containing stage kFastInvReduceStage see inputs below
+// 2^p * 2q at stage p; that round first reduces its elements to [0, q) (inv64 =
+// floor(2^64/q)) and sees inputs below 2^(p - P_LO) * 2q; later rounds count
+// from the earliest start that round can have, kFastInvReduceStage - LOG_E + 1
+// (a bound at least as large as the true one).  Outputs are canonical either
+// way, so the values equal the exact Harvey schedule's.
 template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, bool FASTI = false>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
                       const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq,
@@ -202,7 +203,9 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
     const uint64_t q2 = 2 * q;
     constexpr int E = 1 << LOG_E;
     constexpr uint32_t N = 1u << LOG_N;
-    constexpr bool RED = FASTI && P_LO >= kFastInvReduceStage;
+    constexpr bool RED = FASTI && P_LO <= kFastInvReduceStage && kFastInvReduceStage <= P_HI;
+    constexpr bool AFTER = FASTI && P_LO > kFastInvReduceStage;
+    constexpr int BASE = RED ? P_LO : (AFTER ? kFastInvReduceStage - LOG_E + 1 : 0);
     if constexpr (RED) {
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
@@ -213,7 +216,7 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
         constexpr int half = 1 << r;
         constexpr int nk = E >> (r + 1);
         // bound of this stage's inputs
-        const uint64_t bnd = FASTI ? (q2 << (RED ? p - P_LO : p)) : q2;
+        const uint64_t bnd = FASTI ? (q2 << (p - BASE)) : q2;
         if constexpr (p == LOG_N - 1) {
             const ulonglong2 s = *sptr, sr = *srptr;
             static_for<0, E>([&](auto jt) {
