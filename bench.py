@@ -352,6 +352,7 @@ def run_gpu(args):
                          "ext_product": bench_ext_product(P, stream, cpu=not args.no_cpu),
                          "hybrid_ks": bench_hybrid_ks(P, stream),
                          "widened": bench_widened(P, stream),
+                         "pointwise": bench_pointwise(P, stream),
                          "served_mixed": bench_served(P, stream),
                          "autotune_L24": bench_autotune(P)}
         out = {
@@ -561,6 +562,29 @@ def bench_widened(P, stream, batch=64):
     return res
 
 
+def bench_pointwise(P, stream, polys=64):
+    """Pointwise DCRT ops (DcrtPolynomial::mul_assign / add_mul_assign / add_assign /
+    mul_scalar_assign) on 64 polys of N = 2^16, L = 24 (0.8 GB per operand, beyond
+    L2): HBM GB/s of each against the measured copy peak."""
+    L_, N_ = 24, 1 << 16
+    tab = P.DcrtTable(16, P.ntt_primes(1 << 50, 2 * N_, L_))
+    x, y, z = (P.DeviceBuffer(polys * L_ * N_) for _ in range(3))
+    for i, b in enumerate((x, y, z)):
+        tab.fill_uniform(b, polys, seed=0x70 + i, stream=stream)
+    peak, kind = load_peaks()
+    words = polys * L_ * N_
+    ops = {"mul": (lambda: tab.mul(x, y, polys, stream=stream), 3),
+           "add_mul": (lambda: tab.add_mul(x, y, z, polys, stream=stream), 4),
+           "add": (lambda: tab.add(x, y, polys, stream=stream), 3),
+           "mul_scalar": (lambda: tab.mul_scalar(x, [3] * L_, polys, stream=stream), 2)}
+    res = {"shape": f"{polys} polys x 24 limbs x 2^16", "peak_gbs": peak, "peak_source": kind}
+    for name, (fn, streams) in ops.items():
+        ms = _time_stream(P, stream, fn, 10)
+        gbs = streams * words * 8 / (ms / 1e3) / 1e9
+        res[name] = {"ms": ms, "hbm_gbs": gbs, "frac_of_peak": gbs / peak}
+    return res
+
+
 def run_workload(args):
     """One secondary workload alone (for profiler captures and focused runs)."""
     import primus_b200 as P
@@ -570,6 +594,7 @@ def run_workload(args):
           "ext_product": lambda: bench_ext_product(P, stream, cpu=not args.no_cpu),
           "hybrid_ks": lambda: bench_hybrid_ks(P, stream),
           "widened": lambda: bench_widened(P, stream),
+          "pointwise": lambda: bench_pointwise(P, stream),
           "served_mixed": lambda: bench_served(P, stream),
           "autotune_L24": lambda: bench_autotune(P)}[args.workload]
     print(json.dumps({"workload_name": args.workload, **fn()}))
@@ -735,7 +760,7 @@ def main(argv=None):
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")
     ap.add_argument("--workload", default=None,
                     choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "widened",
-                             "served_mixed", "autotune_L24"],
+                             "pointwise", "served_mixed", "autotune_L24"],
                     help="run only this secondary workload and print its result")
     args = ap.parse_args(argv)
     set_polys(args.polys)

@@ -117,6 +117,9 @@ PG_DEV uint64_t neg_mod(uint64_t a, uint64_t m) { return a == 0 ? 0 : m - a; }
 // output is canonical, so it equals the CPU path's value for any exact method.
 struct Barrett {
     uint64_t q, r0, r1;  // ratio = r1*2^64 + r0
+    // floor(2^(n+62) / q) with n = bitlen(q) when 2 <= n <= 62, else 0: the
+    // factor of the shifted-operand Barrett reduction (barrett_mul)
+    uint64_t mu;
 };
 
 PG_DEV uint64_t barrett_reduce_2limb(uint64_t lo, uint64_t hi, const Barrett& m) {
@@ -138,8 +141,26 @@ PG_DEV uint64_t barrett_reduce_2limb(uint64_t lo, uint64_t hi, const Barrett& m)
     return r >= m.q ? r - m.q : r;
 }
 
+// x mod q for x = hi*2^64 + lo < 2^(n+62), n = bitlen(q) <= 62 (m.mu != 0).
+// Barrett's reduction on the operand shifted right by n-2 bits (Barrett 1986;
+// the pre-shifted form of Harvey's modular-multiplication analysis):
+// c = x >> (n-2) < 2^64 and est = floor(c * mu / 2^64) never exceeds x/q and
+// falls short of it by less than 2.5 (x - c*2^(n-2) < 2^(n-2) <= q/2 and
+// c*(2^(n+62)/q - mu)/2^64 < 1), so x - est*q lies in [0, 3q), below 2^64,
+// and two conditional subtractions make it canonical.  Four 64-bit
+// multiplies per product instead of the nine of the 128-bit ratio form.
+PG_DEV uint64_t barrett_reduce_shifted(uint64_t lo, uint64_t hi, const Barrett& m) {
+    const uint32_t s = 62 - __clzll(m.q);  // n - 2, in [0, 60]
+    const uint64_t c = (lo >> s) | ((hi << 1) << (63 - s));
+    const uint64_t est = mulhi64(c, m.mu);
+    uint64_t r = lo - est * m.q;
+    r = r >= m.q ? r - m.q : r;
+    return r >= m.q ? r - m.q : r;
+}
+
 PG_DEV uint64_t barrett_mul(uint64_t a, uint64_t b, const Barrett& m) {
-    return barrett_reduce_2limb(a * b, mulhi64(a, b), m);
+    const uint64_t lo = a * b, hi = mulhi64(a, b);
+    return m.mu ? barrett_reduce_shifted(lo, hi, m) : barrett_reduce_2limb(lo, hi, m);
 }
 
 PG_DEV uint64_t barrett_mul_add(uint64_t a, uint64_t b, uint64_t c, const Barrett& m) {
@@ -147,7 +168,7 @@ PG_DEV uint64_t barrett_mul_add(uint64_t a, uint64_t b, uint64_t c, const Barret
     uint64_t hi = mulhi64(a, b);
     lo += c;
     hi += (lo < c);
-    return barrett_reduce_2limb(lo, hi, m);
+    return m.mu ? barrett_reduce_shifted(lo, hi, m) : barrett_reduce_2limb(lo, hi, m);
 }
 
 // Counter-based seeded generator (identical to the host generator): a 64-bit

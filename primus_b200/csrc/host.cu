@@ -105,6 +105,9 @@ Barrett h_barrett(uint64_t q) {
     b.q = q;
     b.r0 = r0;
     b.r1 = r1;
+    // shifted-operand Barrett factor floor(2^(n+62) / q), n = bitlen(q)
+    const int n = 64 - __builtin_clzll(q | 1);
+    b.mu = (n >= 2 && n <= 62) ? (uint64_t)((((u128)1) << (n + 62)) / q) : 0;
     return b;
 }
 

@@ -6,6 +6,7 @@
 // side carries precomputed quotients.  The kernels are HBM-bound streams:
 // 16-byte vector accesses, grid sized to a multiple of the SM count.
 #include <algorithm>
+#include <vector>
 
 #include "internal.hpp"
 
@@ -28,7 +29,7 @@ struct PwArgs {
     const uint64_t* y;   // rhs
     const uint64_t* z;   // second rhs / quotients
     const Barrett* bar;  // [L]
-    const uint64_t* scalars;  // [L] (device copy)
+    const uint64_t* scalars;  // [2L] (device copy): scalars, then their Shoup quotients
     uint64_t pairs;      // element pairs in x
     uint64_t rhs_pairs;  // element pairs in one rhs period (L*N/2 when broadcast)
     uint32_t log_n, L;
@@ -55,42 +56,65 @@ PG_DEV uint64_t shoup_quotient(uint64_t w, const Barrett& m) {
 }
 
 template <int OP>
-PG_DEV void pw_elem(uint64_t& x, uint64_t y, uint64_t z, const Barrett& m, uint64_t sc) {
+PG_DEV void pw_elem(uint64_t& x, uint64_t y, uint64_t z, const Barrett& m, uint64_t sc, uint64_t scq) {
     const uint64_t q = m.q;
     if constexpr (OP == PW_MUL) x = barrett_mul(x, y, m);
     if constexpr (OP == PW_ADD_MUL) x = barrett_mul_add(y, z, x, m);
     if constexpr (OP == PW_ADD) x = add_mod(x, y, q);
     if constexpr (OP == PW_SUB) x = sub_mod(x, y, q);
     if constexpr (OP == PW_NEG) x = neg_mod(x, q);
-    if constexpr (OP == PW_MUL_SCALAR) x = barrett_mul(x, sc, m);
-    if constexpr (OP == PW_ADD_MUL_SCALAR) x = barrett_mul_add(y, sc, x, m);
+    if constexpr (OP == PW_MUL_SCALAR) x = shoup_mul(sc, scq, x, q);
+    if constexpr (OP == PW_ADD_MUL_SCALAR) x = add_mod(x, shoup_mul(sc, scq, y, q), q);
     if constexpr (OP == PW_MUL_PREPARED) x = shoup_mul(y, z, x, q);
     if constexpr (OP == PW_SHOUP_PREPARE) x = shoup_quotient(y, m);
 }
 
-// grid: y over polys, x over the L*N/2 element pairs of one poly (32-bit index)
+// pairs per thread: the multiplying ops hold more registers (fewer resident
+// threads), so each thread issues the loads of two pairs before computing to
+// keep as many bytes in flight per SM as the light ops do
+template <int OP>
+__host__ __device__ constexpr int pw_per_thread() {
+    return (OP == PW_MUL || OP == PW_ADD_MUL || OP == PW_MUL_PREPARED || OP == PW_SHOUP_PREPARE) ? 2 : 1;
+}
+
+// grid: y over polys, x over the L*N/2 element pairs of one poly (32-bit
+// index); CTA b covers pairs [b*256*PER, (b+1)*256*PER), thread t of it the
+// pairs t, t+256, ... (coalesced)
 template <int OP>
 __global__ void __launch_bounds__(256) pw_kernel(PwArgs a) {
+    constexpr int PER = pw_per_thread<OP>();
+    constexpr bool SC = OP == PW_MUL_SCALAR || OP == PW_ADD_MUL_SCALAR;
     const uint32_t pp = (uint32_t)((a.L << a.log_n) >> 1);  // pairs per poly
     const uint64_t polys = a.pairs / pp;
     for (uint64_t p = blockIdx.y; p < polys; p += gridDim.y) {
         ulonglong2* xp = reinterpret_cast<ulonglong2*>(a.x) + p * pp;
         const uint64_t roff = a.rhs_pairs ? 0 : p * pp;
-        for (uint32_t ix = blockIdx.x * blockDim.x + threadIdx.x; ix < pp; ix += gridDim.x * blockDim.x) {
-            const uint32_t limb = (2 * ix) >> a.log_n;
-            const Barrett m = a.bar[limb];
-            const uint64_t ri = roff + ix;
-            ulonglong2 x = xp[ix];
-            ulonglong2 y = make_ulonglong2(0, 0), z = make_ulonglong2(0, 0);
-            if constexpr (OP != PW_NEG && OP != PW_MUL_SCALAR)
-                y = __ldg(reinterpret_cast<const ulonglong2*>(a.y) + ri);
-            if constexpr (OP == PW_ADD_MUL || OP == PW_MUL_PREPARED)
-                z = __ldg(reinterpret_cast<const ulonglong2*>(a.z) + ri);
-            const uint64_t sc = (OP == PW_MUL_SCALAR || OP == PW_ADD_MUL_SCALAR) ? a.scalars[limb] : 0;
-            uint64_t x0 = x.x, x1 = x.y;
-            pw_elem<OP>(x0, y.x, z.x, m, sc);
-            pw_elem<OP>(x1, y.y, z.y, m, sc);
-            xp[ix] = make_ulonglong2(x0, x1);
+        for (uint32_t i0 = blockIdx.x * (256 * PER) + threadIdx.x; i0 < pp; i0 += gridDim.x * (256 * PER)) {
+            ulonglong2 x[PER], y[PER], z[PER];
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const uint32_t ix = i0 + 256 * k;
+                x[k] = y[k] = z[k] = make_ulonglong2(0, 0);
+                if (ix < pp) {
+                    x[k] = xp[ix];
+                    if constexpr (OP != PW_NEG && OP != PW_MUL_SCALAR)
+                        y[k] = __ldg(reinterpret_cast<const ulonglong2*>(a.y) + roff + ix);
+                    if constexpr (OP == PW_ADD_MUL || OP == PW_MUL_PREPARED)
+                        z[k] = __ldg(reinterpret_cast<const ulonglong2*>(a.z) + roff + ix);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const uint32_t ix = i0 + 256 * k;
+                if (ix >= pp) break;
+                const uint32_t limb = (2 * ix) >> a.log_n;
+                const Barrett m = a.bar[limb];
+                const uint64_t sc = SC ? a.scalars[limb] : 0, scq = SC ? a.scalars[a.L + limb] : 0;
+                uint64_t x0 = x[k].x, x1 = x[k].y;
+                pw_elem<OP>(x0, y[k].x, z[k].x, m, sc, scq);
+                pw_elem<OP>(x1, y[k].y, z[k].y, m, sc, scq);
+                xp[ix] = make_ulonglong2(x0, x1);
+            }
         }
     }
 }
@@ -153,13 +177,18 @@ static int launch_pw(const pg_ntt_table* t, uint64_t* x, const uint64_t* y, cons
     uint64_t* d_sc = nullptr;
     if (OP == PW_MUL_SCALAR || OP == PW_ADD_MUL_SCALAR) {
         if (!h_scalars) return set_error(PG_ERR_INVALID_ARGUMENT, "scalars is NULL");
-        for (uint32_t l = 0; l < t->L; ++l)
+        // pageable source: the copy below completes before the call returns
+        std::vector<uint64_t> sq(2 * (size_t)t->L);
+        for (uint32_t l = 0; l < t->L; ++l) {
             if (h_scalars[l] >= t->moduli[l]) return set_error(PG_ERR_INVALID_ARGUMENT, "scalar not below its modulus");
-        PG_CUDA(scratch_alloc((void**)&d_sc, t->L * sizeof(uint64_t), st));
-        PG_CUDA(cudaMemcpyAsync(d_sc, h_scalars, t->L * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            sq[l] = h_scalars[l];
+            sq[t->L + l] = h_shoup_quotient(h_scalars[l], t->moduli[l]);
+        }
+        PG_CUDA(scratch_alloc((void**)&d_sc, sq.size() * sizeof(uint64_t), st));
+        PG_CUDA(cudaMemcpyAsync(d_sc, sq.data(), sq.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         a.scalars = d_sc;
     }
-    pw_kernel<OP><<<grid2((uint64_t)t->L * t->n / 2, polys), 256, 0, st>>>(a);
+    pw_kernel<OP><<<grid2((uint64_t)t->L * t->n / 2 / pw_per_thread<OP>(), polys), 256, 0, st>>>(a);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (d_sc) scratch_free(d_sc, st);

@@ -106,3 +106,47 @@ def test_butterfly_mul_factor(gpu):
             ea, eb = O.butterfly_mul_factor(a[p, l], s[p, l], w[0, l], q)
             assert np.array_equal(da.numpy(a.shape)[p, l], ea)
             assert np.array_equal(db.numpy(a.shape)[p, l], eb)
+
+
+@pytest.mark.parametrize("bits", [15, 31, 45, 55, 60, 62])
+def test_products_across_modulus_widths(gpu, bits):
+    """The multiply paths hold for every modulus width the table accepts, with
+    operands at the extremes (0, 1, q-1) mixed into uniform residues."""
+    log_n, L, polys = 10, 2, 2
+    n = 1 << log_n
+    moduli = O.ntt_primes(1 << bits, 2 << log_n, L)
+    tab = gpu.DcrtTable(log_n, moduli)
+    rng = np.random.default_rng(bits)
+
+    def operand(s):
+        v = np.stack([O.uniform_rns(1000 * bits + s, p * L, moduli, n) for p in range(polys)])
+        for l, q in enumerate(moduli):
+            pick = rng.integers(0, 4, size=(polys, n))
+            v[:, l] = np.where(pick == 0, np.uint64(q - 1), np.where(pick == 1, np.uint64(0), v[:, l]))
+        return v
+
+    x, y, z = operand(1), operand(2), operand(3)
+    d = gpu.DeviceBuffer.from_numpy(x)
+    tab.mul(d, gpu.DeviceBuffer.from_numpy(y), polys)
+    assert np.array_equal(d.numpy(x.shape), per_limb(O.mul, x, y, moduli=moduli))
+    d = gpu.DeviceBuffer.from_numpy(x)
+    tab.add_mul(d, gpu.DeviceBuffer.from_numpy(y), gpu.DeviceBuffer.from_numpy(z), polys)
+    exp = x.copy()
+    for p in range(polys):
+        for l, q in enumerate(moduli):
+            exp[p, l] = O.add_mul(x[p, l], y[p, l], z[p, l], q)
+    assert np.array_equal(d.numpy(x.shape), exp)
+    for sc in ([q - 1 for q in moduli], [1, 0], [int(O.uniform(bits, l, q, 1)[0]) for l, q in enumerate(moduli)]):
+        d = gpu.DeviceBuffer.from_numpy(x)
+        tab.mul_scalar(d, sc, polys)
+        exp = x.copy()
+        for p in range(polys):
+            for l, q in enumerate(moduli):
+                exp[p, l] = O.mul_scalar(x[p, l], sc[l], q)
+        assert np.array_equal(d.numpy(x.shape), exp)
+        d = gpu.DeviceBuffer.from_numpy(x)
+        tab.add_mul_scalar(d, gpu.DeviceBuffer.from_numpy(y), sc, polys)
+        for p in range(polys):
+            for l, q in enumerate(moduli):
+                exp[p, l] = O.add_mul_scalar(x[p, l], y[p, l], sc[l], q)
+        assert np.array_equal(d.numpy(x.shape), exp)
