@@ -168,7 +168,7 @@ int pg_ntt_inverse(const pg_ntt_table *table, uint64_t *d_data, size_t polys, in
 int pg_ntt_forward_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
 int pg_ntt_inverse_host(const pg_ntt_table *table, uint64_t *h_data, size_t polys, int lazy);
 /* NTT of coeff*X^degree into every limb (coeff < every q), of X^degree and of
- * -X^degree.  Replaces transform_monomial / transform_coeff_one_monomial /
+ * -X^degree; any degree (exponents mod 2N, X^N = -1).  Replaces transform_monomial / transform_coeff_one_monomial /
  * transform_coeff_minus_one_monomial (primitive.rs:298-397, dcrt/mod.rs:100-128). */
 int pg_ntt_monomial(const pg_ntt_table *table, uint64_t coeff, size_t degree, uint64_t *d_out,
                     void *stream);
@@ -350,6 +350,30 @@ size_t pg_glwe_automorphism_workspace_size(const pg_ntt_table *table, const pg_g
 int pg_glwe_automorphism(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
                          uint64_t degree, const uint64_t *d_key, const uint64_t *d_c_in, uint64_t *d_c_out,
                          size_t batch, void *d_workspace, size_t workspace_bytes, void *stream);
+/* Field trace: DcrtGlweTraceKey::trace_inplace
+ * (primus_fhe_core/src/trace/glwe/dcrt.rs:84-108): c_out = c_in, then
+ * c_out += sigma_d(c_out) for d = N+1, N/2+1, .., 3 (log2 N automorphisms).
+ * With reverse != 0, DcrtGlweRevTraceKey::trace_inplace (trace/glwe/rev.rs:79-115):
+ * d = 3, 5, .., N+1, c_out *= 2^-1 mod q_l before each automorphism.  keys:
+ * log2(N) automorphism keys in the order applied, each [k][d][k+1][L][N];
+ * c_in, c_out: [batch][k+1][L][N] NTT domain, the same buffer or disjoint. */
+size_t pg_glwe_trace_workspace_size(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                                    size_t batch);
+int pg_glwe_trace(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k, const uint64_t *d_keys,
+                  int reverse, const uint64_t *d_c_in, uint64_t *d_c_out, size_t batch, void *d_workspace,
+                  size_t workspace_bytes, void *stream);
+/* Coefficient expansion: DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace
+ * (primus_fhe_core/src/expand_coeff/glwe/dcrt.rs:235-287; count = N is
+ * expand_coefficients_inplace).  count: a power of two <= N; keys as for the
+ * forward trace (degrees N+1, N/2+1, ..; the first log2(count) are read);
+ * c_in: one ciphertext [k+1][L][N]; out: [count][k+1][L][N] (c_in may be out's
+ * first slot).  For an input encrypting m, output j encrypts
+ * sum_i m[j + count*i] X^(count*i) (m[j] alone when count = N). */
+size_t pg_glwe_expand_workspace_size(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                                     size_t count);
+int pg_glwe_expand_coefficients(const pg_ntt_table *table, const pg_gadget_basis *basis, uint32_t k,
+                                const uint64_t *d_keys, size_t count, const uint64_t *d_c_in, uint64_t *d_out,
+                                void *d_workspace, size_t workspace_bytes, void *stream);
 /* BFV-style GLWE decryption through fast base conversion:
  * DcrtGlweSecretKey::decrypt_inplace (primus_fhe_core/src/secret_key/glwe.rs:782-837).
  * phase = b - sum a_i s_i (NTT domain), inverse NTT, x [t gamma]_q, fast

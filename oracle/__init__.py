@@ -128,6 +128,8 @@ def lib():
             "orc_bfv_delta": (None, [C.c_void_p, C.c_uint64, u64p]),
             "orc_ntt_auto_perm": (None, [C.c_uint32, C.c_uint64, u32p]),
             "orc_glwe_automorphism": (None, [C.c_void_p, C.c_uint32, C.c_uint64, u64p, u64p, u64p]),
+            "orc_glwe_trace": (None, [C.c_void_p, C.c_uint32, u64p, C.c_int, u64p, u64p]),
+            "orc_glwe_expand": (None, [C.c_void_p, C.c_uint32, u64p, C.c_size_t, u64p, u64p]),
             "orc_cdt_table": (C.c_uint32, [C.c_double, u64p, C.c_uint32]),
             "orc_cdt_sample": (C.c_int64, [u64p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
             "orc_glwe_encrypt_cdt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, u64p, C.c_double, C.c_uint64,
@@ -500,6 +502,18 @@ class Lattice:
         """DcrtGlweAutoKey::automorphism_inplace: NTT-domain GLWE in and out."""
         out = np.zeros((k + 1) * self.L * self.n, np.uint64)
         lib().orc_glwe_automorphism(self.pctx, k, degree, p64(u64(key)), p64(u64(ct_in)), p64(out))
+        return out
+
+    def trace(self, k, keys, ct_in, reverse=False):
+        """DcrtGlweTraceKey / DcrtGlweRevTraceKey::trace_inplace (keys in the order applied)."""
+        out = np.zeros((k + 1) * self.L * self.n, np.uint64)
+        lib().orc_glwe_trace(self.pctx, k, p64(u64(keys)), int(reverse), p64(u64(ct_in)), p64(out))
+        return out
+
+    def expand(self, k, keys, count, ct_in):
+        """DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace: [count][k+1][L][N]."""
+        out = np.zeros(count * (k + 1) * self.L * self.n, np.uint64)
+        lib().orc_glwe_expand(self.pctx, k, p64(u64(keys)), count, p64(u64(ct_in)), p64(out))
         return out
 
     def encrypt_cdt(self, k, sk_ntt, msg, scale, seed, stream0, index, sigma=3.2):

@@ -1569,6 +1569,79 @@ void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree
     free(perm);
 }
 
+/* DcrtGlweTraceKey::trace_inplace (primus_fhe_core/src/trace/glwe/dcrt.rs:84-108):
+ * result = ct; for each key: result += sigma(result), degrees N+1, N/2+1, .., 3
+ * (keys built at :66-71).  DcrtGlweRevTraceKey::trace_inplace
+ * (trace/glwe/rev.rs:79-115): degrees 3, 5, .., N+1 (:41-45), and before each
+ * automorphism the ciphertext is multiplied by 2^-1 = (q+1)/2 mod q (:47-53, :101-107). */
+void orc_glwe_trace(const orc_lattice_ctx *c, uint32_t k, const uint64_t *keys, int reverse,
+                    const uint64_t *ct_in, uint64_t *ct_out) {
+    const size_t n = c->n;
+    const uint32_t L = c->L, log_n = (uint32_t)__builtin_ctzll(n);
+    const size_t poly = (size_t)L * n, glwe = (size_t)(k + 1) * poly;
+    const size_t key_len = (size_t)k * c->basis->decompose_length * glwe;
+    uint64_t *tmp = malloc(glwe * 8);
+    memmove(ct_out, ct_in, glwe * 8);
+    for (uint32_t r = 0; r < log_n; ++r) {
+        const uint64_t degree = reverse ? ((uint64_t)2 << r) + 1 : (uint64_t)(n >> r) + 1;
+        if (reverse)
+            for (uint32_t i = 0; i <= k; ++i)
+                for (uint32_t l = 0; l < L; ++l) {
+                    const uint64_t q = c->tables[l]->q, h = (q + 1) >> 1;
+                    orc_mul_factor_assign(ct_out + (size_t)i * poly + (size_t)l * n, h, orc_shoup_quotient(h, q),
+                                          n, q);
+                }
+        orc_glwe_automorphism(c, k, degree, keys + (size_t)r * key_len, ct_out, tmp);
+        for (uint32_t i = 0; i <= k; ++i)
+            for (uint32_t l = 0; l < L; ++l)
+                orc_add_assign(ct_out + (size_t)i * poly + (size_t)l * n, tmp + (size_t)i * poly + (size_t)l * n,
+                               n, c->tables[l]->q);
+    }
+    free(tmp);
+}
+
+/* DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace
+ * (primus_fhe_core/src/expand_coeff/glwe/dcrt.rs:235-287): result[0] = ct *
+ * count^-1 mod q_l (inv_count_residues, :209-232), then level i = 0 ..
+ * log2(count)-1 with the key of degree N/2^i + 1 and the Shoup factor
+ * NTT(X^(2N - 2^i)) (precompute_monomial_factors, :181-207): for j < 2^i,
+ * (result[j], result[j + 2^i]) = (a + sigma(a), (a - sigma(a)) * factor), a = result[j]. */
+void orc_glwe_expand(const orc_lattice_ctx *c, uint32_t k, const uint64_t *keys, size_t count,
+                     const uint64_t *ct_in, uint64_t *out) {
+    const size_t n = c->n;
+    const uint32_t L = c->L;
+    const size_t poly = (size_t)L * n, glwe = (size_t)(k + 1) * poly;
+    const size_t key_len = (size_t)k * c->basis->decompose_length * glwe;
+    const uint32_t log_d = (uint32_t)__builtin_ctzll(count);
+    memmove(out, ct_in, glwe * 8);
+    for (uint32_t l = 0; l < L; ++l) {
+        const uint64_t q = c->tables[l]->q, inv = orc_invmod(count % q, q), invq = orc_shoup_quotient(inv, q);
+        for (uint32_t i = 0; i <= k; ++i) orc_mul_factor_assign(out + (size_t)i * poly + (size_t)l * n, inv, invq, n, q);
+    }
+    uint64_t *tmp = malloc(glwe * 8), *w = malloc(poly * 8), *wq = malloc(poly * 8);
+    for (uint32_t lev = 0; lev < log_d; ++lev) {
+        const size_t half = (size_t)1 << lev;
+        for (uint32_t l = 0; l < L; ++l) {
+            orc_ntt_coeff_one_monomial(c->tables[l], 2 * n - half, w + (size_t)l * n);
+            for (size_t x = 0; x < n; ++x) wq[(size_t)l * n + x] = orc_shoup_quotient(w[(size_t)l * n + x], c->tables[l]->q);
+        }
+        const uint64_t degree = (uint64_t)(n >> lev) + 1;
+        for (size_t j = 0; j < half; ++j) {
+            uint64_t *a = out + j * glwe, *b = out + (j + half) * glwe;
+            orc_glwe_automorphism(c, k, degree, keys + (size_t)lev * key_len, a, tmp);
+            for (uint32_t i = 0; i <= k; ++i)
+                for (uint32_t l = 0; l < L; ++l) {
+                    const size_t o = (size_t)i * poly + (size_t)l * n;
+                    orc_butterfly_mul_factor(a + o, tmp + o, w + (size_t)l * n, wq + (size_t)l * n, b + o, n,
+                                             c->tables[l]->q);
+                }
+        }
+    }
+    free(tmp);
+    free(w);
+    free(wq);
+}
+
 /* ======================================================================
  * Encryption with the CDT Gaussian sampler (reproducible on the device)
  * ====================================================================== */

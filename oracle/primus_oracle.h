@@ -294,6 +294,19 @@ void orc_ntt_auto_perm(uint32_t log_n, uint64_t degree, uint32_t *perm);
  * domain; key = k GLevs [k][d][k+1][L][N] (GLev of sigma(s_i) under s) */
 void orc_glwe_automorphism(const orc_lattice_ctx *c, uint32_t k, uint64_t degree, const uint64_t *key,
                            const uint64_t *ct_in, uint64_t *ct_out);
+/* Field trace by log2(N) automorphisms: DcrtGlweTraceKey::trace_inplace
+ * (primus_fhe_core/src/trace/glwe/dcrt.rs:84-108; degrees N+1, N/2+1, .., 3)
+ * or, with reverse != 0, DcrtGlweRevTraceKey::trace_inplace (trace/glwe/rev.rs:79-115;
+ * degrees 3, 5, .., N+1, each step halving first).  keys: log2(N) automorphism
+ * keys in the order applied, each [k][d][k+1][L][N]. */
+void orc_glwe_trace(const orc_lattice_ctx *c, uint32_t k, const uint64_t *keys, int reverse,
+                    const uint64_t *ct_in, uint64_t *ct_out);
+/* Coefficient expansion: DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace
+ * (primus_fhe_core/src/expand_coeff/glwe/dcrt.rs:235-287).  keys as for the
+ * forward trace (degrees N+1, N/2+1, ..; the first log2(count) are used);
+ * out: [count][k+1][L][N]. */
+void orc_glwe_expand(const orc_lattice_ctx *c, uint32_t k, const uint64_t *keys, size_t count,
+                     const uint64_t *ct_in, uint64_t *out);
 
 /* ---- encryption with the device-reproducible sampler (CDT Gaussian) ----
  * Discrete Gaussian over [-B, B], B = ceil(24 sigma) (the reference's bound,

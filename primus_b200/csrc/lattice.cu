@@ -505,3 +505,130 @@ int pg_ext_product_noalloc(const pg_ntt_table* t, const pg_gadget_basis* g, uint
 }
 
 }  // extern "C"
+
+// ---- field trace and coefficient expansion: sums of automorphisms
+// (primus_fhe_core/src/trace, primus_fhe_core/src/expand_coeff)
+namespace {
+
+// one automorphism key: k GLevs [k][d][k+1][L][N]
+size_t auto_key_words(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k) {
+    return (size_t)k * gadget_d(g) * (k + 1) * t->L * t->n;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// ciphertexts per automorphism call inside an expansion level, bounding the
+// workspace of the late levels (2^i ciphertexts each)
+constexpr size_t kExpandChunk = 256;
+
+size_t expand_chunk(size_t count) { return std::max<size_t>(1, std::min(count / 2, kExpandChunk)); }
+
+bool ranges_overlap(const uint64_t* a, size_t na, const uint64_t* b, size_t nb) { return a < b + nb && b < a + na; }
+
+}  // namespace
+
+extern "C" {
+
+size_t pg_glwe_trace_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, size_t batch) {
+    if (!t || !g) return 0;
+    return round256(batch * (k + 1) * (size_t)t->L * t->n * 8) + pg_glwe_automorphism_workspace_size(t, g, k, batch);
+}
+
+// DcrtGlweTraceKey::trace_inplace (primus_fhe_core/src/trace/glwe/dcrt.rs:84-108):
+// out = in, then out += sigma_d(out) for d = N+1, N/2+1, .., 3; with reverse,
+// DcrtGlweRevTraceKey::trace_inplace (trace/glwe/rev.rs:79-115): d = 3, 5, ..,
+// N+1 and out *= 2^-1 before each automorphism.  Each step is one batched
+// automorphism and one batched add over every ciphertext.
+int pg_glwe_trace(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_keys, int reverse,
+                  const uint64_t* d_in, uint64_t* d_out, size_t batch, void* d_ws, size_t ws_size, void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (batch == 0) return PG_OK;
+    if (!d_keys || !d_in || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (k == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k must be at least 1");
+    const size_t glwe = (size_t)(k + 1) * t->L * t->n, polys = batch * (k + 1);
+    if (d_in != d_out && ranges_overlap(d_in, batch * glwe, d_out, batch * glwe))
+        return set_error(PG_ERR_INVALID_ARGUMENT, "input and output must be the same buffer or not overlap");
+    cudaStream_t st = (cudaStream_t)stream;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, pg_glwe_trace_workspace_size(t, g, k, batch), st);
+    if (rc) return rc;
+    uint64_t* tmp = (uint64_t*)w.ptr;
+    void* aws = (char*)w.ptr + round256(batch * glwe * 8);
+    const size_t aws_size = pg_glwe_automorphism_workspace_size(t, g, k, batch);
+    if (d_in != d_out) PG_CUDA(cudaMemcpyAsync(d_out, d_in, batch * glwe * 8, cudaMemcpyDeviceToDevice, st));
+    std::vector<uint64_t> half(t->L);
+    for (uint32_t l = 0; l < t->L; ++l) half[l] = (t->moduli[l] + 1) >> 1;  // 2^-1 mod q_l (rev.rs:47-53)
+    const size_t kw = auto_key_words(t, g, k);
+    for (uint32_t r = 0; r < t->log_n; ++r) {
+        const uint64_t degree = reverse ? ((uint64_t)2 << r) + 1 : (uint64_t)(t->n >> r) + 1;
+        if (reverse && (rc = pg_dcrt_mul_scalar(t, d_out, half.data(), polys, stream))) return rc;
+        rc = pg_glwe_automorphism(t, g, k, degree, d_keys + r * kw, d_out, tmp, batch, aws, aws_size, stream);
+        if (rc) return rc;
+        rc = pg_dcrt_add(t, d_out, tmp, polys, polys, stream);
+        if (rc) return rc;
+    }
+    return PG_OK;
+}
+
+size_t pg_glwe_expand_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, size_t count) {
+    if (!t || !g) return 0;
+    const size_t c = expand_chunk(count), LN = (size_t)t->L * t->n;
+    return round256(c * (k + 1) * LN * 8) + round256(2 * LN * 8) + pg_glwe_automorphism_workspace_size(t, g, k, c);
+}
+
+// DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace
+// (primus_fhe_core/src/expand_coeff/glwe/dcrt.rs:235-287): out[0] = in *
+// count^-1 (:209-232); level i < log2(count) applies the key of degree
+// N/2^i + 1 to out[0 .. 2^i) as batched automorphisms (at most 256 per call)
+// and one batched butterfly (out[j], out[j + 2^i]) = (a + sigma(a),
+// (a - sigma(a)) * NTT(X^(2N - 2^i))) (:181-207).  The reference's levels
+// run their 2^i pairs one by one on rayon workers (:341-412); here each level
+// is a handful of launches over all of its ciphertexts.
+int pg_glwe_expand_coefficients(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_keys,
+                                size_t count, const uint64_t* d_in, uint64_t* d_out, void* d_ws, size_t ws_size,
+                                void* stream) {
+    int rc = check_compat(t, g);
+    if (rc) return rc;
+    if (!d_keys || !d_in || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (k == 0) return set_error(PG_ERR_INVALID_ARGUMENT, "k must be at least 1");
+    if (count == 0 || (count & (count - 1)) || count > t->n)
+        return set_error(PG_ERR_INVALID_ARGUMENT, "count must be a power of two no larger than N");
+    const size_t LN = (size_t)t->L * t->n, glwe = (size_t)(k + 1) * LN;
+    if (d_in != d_out && ranges_overlap(d_in, glwe, d_out, count * glwe))
+        return set_error(PG_ERR_INVALID_ARGUMENT, "input must be the first output slot or not overlap the output");
+    cudaStream_t st = (cudaStream_t)stream;
+    Workspace w;
+    rc = get_workspace(w, d_ws, ws_size, pg_glwe_expand_workspace_size(t, g, k, count), st);
+    if (rc) return rc;
+    const size_t chunk = expand_chunk(count);
+    uint64_t* tmp = (uint64_t*)w.ptr;
+    uint64_t* fw = (uint64_t*)((char*)w.ptr + round256(chunk * glwe * 8));
+    uint64_t* fwq = fw + LN;
+    void* aws = (char*)fw + round256(2 * LN * 8);
+    const size_t aws_size = pg_glwe_automorphism_workspace_size(t, g, k, chunk);
+    if (d_in != d_out) PG_CUDA(cudaMemcpyAsync(d_out, d_in, glwe * 8, cudaMemcpyDeviceToDevice, st));
+    std::vector<uint64_t> inv(t->L);
+    for (uint32_t l = 0; l < t->L; ++l) inv[l] = h_invmod(count % t->moduli[l], t->moduli[l]);
+    rc = pg_dcrt_mul_scalar(t, d_out, inv.data(), k + 1, stream);
+    if (rc) return rc;
+    const size_t kw = auto_key_words(t, g, k);
+    for (uint32_t lev = 0; (size_t(1) << lev) < count; ++lev) {
+        const size_t half = (size_t)1 << lev;
+        if ((rc = pg_ntt_coeff_one_monomial(t, 2 * t->n - half, fw, stream))) return rc;
+        if ((rc = pg_dcrt_shoup_prepare(t, fw, fwq, 1, stream))) return rc;
+        const uint64_t degree = (uint64_t)(t->n >> lev) + 1;
+        for (size_t c0 = 0; c0 < half; c0 += chunk) {
+            const size_t m = std::min(chunk, half - c0);
+            rc = pg_glwe_automorphism(t, g, k, degree, d_keys + lev * kw, d_out + c0 * glwe, tmp, m, aws, aws_size,
+                                      stream);
+            if (rc) return rc;
+            rc = pg_dcrt_butterfly_mul_factor(t, d_out + c0 * glwe, tmp, fw, fwq, d_out + (half + c0) * glwe,
+                                              m * (k + 1), stream);
+            if (rc) return rc;
+        }
+    }
+    return PG_OK;
+}
+
+}  // extern "C"

@@ -308,7 +308,7 @@ __global__ void monomial_kernel(uint64_t* out, const ulonglong2* __restrict__ or
 static int launch_monomial(const pg_ntt_table* t, uint64_t coeff, size_t degree, uint64_t* d_out, int kind,
                            cudaStream_t st) {
     if (!t || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL table or output");
-    if (degree >= t->n) return set_error(PG_ERR_INVALID_ARGUMENT, "degree must be below N");
+    // any degree: exponents are taken mod 2N (X^N = -1), as primitive.rs:319 masks them
     const size_t total = t->n * t->L;
     const unsigned threads = 256;
     const unsigned blocks = (unsigned)std::min<size_t>((total + threads - 1) / threads, 148 * 16);

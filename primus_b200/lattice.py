@@ -161,6 +161,26 @@ def glwe_automorphism(table, basis: GadgetBasis, k: int, degree: int, key: Devic
          _sh(stream))
 
 
+def glwe_trace(table, basis: GadgetBasis, k: int, keys: DeviceBuffer, c_in: DeviceBuffer, c_out: DeviceBuffer,
+               batch: int, reverse: bool = False, workspace: DeviceBuffer | None = None, stream=None):
+    """DcrtGlweTraceKey::trace_inplace (reverse=False; keys of degrees N+1, N/2+1, .., 3)
+    or DcrtGlweRevTraceKey::trace_inplace (reverse=True; degrees 3, 5, .., N+1),
+    keys concatenated in the order applied."""
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_glwe_trace", table.h, basis.h, k, keys.ptr, int(bool(reverse)), c_in.ptr, c_out.ptr, batch, ws, wsb,
+         _sh(stream))
+
+
+def glwe_expand_coefficients(table, basis: GadgetBasis, k: int, keys: DeviceBuffer, count: int, c_in: DeviceBuffer,
+                             out: DeviceBuffer, workspace: DeviceBuffer | None = None, stream=None):
+    """DcrtGlweExpandCoeffKey::expand_partial_coefficients_inplace: out[count][k+1][L][N]."""
+    ws = workspace.ptr if workspace is not None else None
+    wsb = workspace.count * 8 if workspace is not None else 0
+    call("pg_glwe_expand_coefficients", table.h, basis.h, k, keys.ptr, count, c_in.ptr, out.ptr, ws, wsb,
+         _sh(stream))
+
+
 def glev_mac_crt_poly(table, basis: GadgetBasis, k: int, acc: DeviceBuffer, glev: DeviceBuffer,
                       crt_poly: DeviceBuffer, stream=None):
     call("pg_glev_mac_crt_poly", table.h, basis.h, k, acc.ptr, glev.ptr, crt_poly.ptr, None, 0, _sh(stream))

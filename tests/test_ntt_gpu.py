@@ -190,11 +190,13 @@ def test_monomials(gpu, log_n):
     tab = gpu.DcrtTable(log_n, moduli)
     refs = [O.NttTable(log_n, q) for q in moduli]
     out = np.zeros(2 * n, np.uint64)
-    for coeff, deg in [(5, min(7, n - 1)), (1, n - 1), (0, 1), (123456789, 0), (moduli[0] - 1, 1)]:
+    # degrees at and above N wrap mod 2N with X^N = -1 (primitive.rs:319 masks the exponent)
+    for coeff, deg in [(5, min(7, n - 1)), (1, n - 1), (0, 1), (123456789, 0), (moduli[0] - 1, 1), (5, n + 3),
+                       (moduli[0] - 1, 2 * n - 1), (1, 3 * n + 5)]:
         tab.transform_monomial(coeff, deg, out)
         exp = np.concatenate([r.monomial(coeff, deg) for r in refs])
         assert np.array_equal(out, exp), (coeff, deg)
-    for deg in (0, 1, n - 1):
+    for deg in (0, 1, n - 1, n, 2 * n - 1, 5 * n + 1):
         tab.transform_coeff_one_monomial(deg, out)
         assert np.array_equal(out, np.concatenate([r.coeff_one_monomial(deg) for r in refs]))
         tab.transform_coeff_minus_one_monomial(deg, out)
