@@ -353,6 +353,7 @@ def run_gpu(args):
                          "hybrid_ks": bench_hybrid_ks(P, stream),
                          "widened": bench_widened(P, stream),
                          "pointwise": bench_pointwise(P, stream),
+                         "expand": bench_expand(P, stream),
                          "served_mixed": bench_served(P, stream),
                          "autotune_L24": bench_autotune(P)}
         out = {
@@ -562,6 +563,51 @@ def bench_widened(P, stream, batch=64):
     return res
 
 
+def bench_expand(P, stream, cpu=False):
+    """Coefficient expansion and field trace on the reference benchmark's shapes
+    (primus_fhe_core/benches/expand_coeff.rs: k = 2, two primes < 2^50,
+    log_basis 20, N = 2^10, 2^11, 2^12, full expansion count = N): device time of
+    one expansion (N-1 automorphisms in log2 N levels) and of a trace."""
+    import time
+    res = {"shape": "k=2, L=2 primes < 2^50, log_basis 20, count = N"}
+    k = 2
+    for log_n in (10, 11, 12):
+        n = 1 << log_n
+        moduli = P.ntt_primes(1 << 50, 2 << 12, 2)
+        tab = P.DcrtTable(log_n, moduli)
+        g = P.GadgetBasis(P.RnsBase(moduli), 20)
+        glwe = (k + 1) * 2 * n
+        keys = P.DeviceBuffer(log_n * k * g.d * glwe)
+        tab.fill_uniform(keys, log_n * k * g.d * (k + 1), seed=0x90 + log_n, stream=stream)
+        ct = P.DeviceBuffer(glwe)
+        tab.fill_uniform(ct, k + 1, seed=0xA0 + log_n, stream=stream)
+        out = P.DeviceBuffer(n * glwe)
+        ws = P.DeviceBuffer(P.lattice.nat.lib().pg_glwe_expand_workspace_size(tab.h, g.h, k, n) // 8 + 1)
+        ms = _time_stream(P, stream, lambda: P.glwe_expand_coefficients(tab, g, k, keys, n, ct, out, workspace=ws,
+                                                                        stream=stream), 3)
+        tb = 64
+        cts = P.DeviceBuffer(tb * glwe)
+        tab.fill_uniform(cts, tb * (k + 1), seed=0xB0 + log_n, stream=stream)
+        tout = P.DeviceBuffer(tb * glwe)
+        tws = P.DeviceBuffer(P.lattice.nat.lib().pg_glwe_trace_workspace_size(tab.h, g.h, k, tb) // 8 + 1)
+        ms_tr = _time_stream(P, stream, lambda: P.glwe_trace(tab, g, k, keys, cts, tout, tb, workspace=tws,
+                                                             stream=stream), 3)
+        res[f"N=2^{log_n}"] = {"expand_ms": ms, "automorphisms": n - 1, "digits": g.d,
+                               "us_per_automorphism": ms * 1e3 / (n - 1),
+                               "trace_batch64_us_per_ciphertext": ms_tr * 1e3 / tb}
+        if cpu and log_n == 10:
+            import numpy as np
+            import oracle as O
+            lat = O.Lattice(O.DcrtTable(log_n, moduli), O.RnsBase(moduli), O.GadgetBasis(O.RnsBase(moduli), 20))
+            hk = keys.numpy()[: k * g.d * glwe * log_n].astype(np.uint64)
+            t0 = time.perf_counter()
+            lat.expand(k, hk, n, ct.numpy())
+            dt = time.perf_counter() - t0
+            res[f"N=2^{log_n}"]["cpu_port_expand_ms"] = dt * 1e3
+            res[f"N=2^{log_n}"]["cpu_port_sample"] = "one full expansion, oracle restatement, 1 thread"
+    return res
+
+
 def bench_pointwise(P, stream, polys=64):
     """Pointwise DCRT ops (DcrtPolynomial::mul_assign / add_mul_assign / add_assign /
     mul_scalar_assign) on 64 polys of N = 2^16, L = 24 (0.8 GB per operand, beyond
@@ -595,6 +641,7 @@ def run_workload(args):
           "hybrid_ks": lambda: bench_hybrid_ks(P, stream),
           "widened": lambda: bench_widened(P, stream),
           "pointwise": lambda: bench_pointwise(P, stream),
+          "expand": lambda: bench_expand(P, stream, cpu=not args.no_cpu),
           "served_mixed": lambda: bench_served(P, stream),
           "autotune_L24": lambda: bench_autotune(P)}[args.workload]
     print(json.dumps({"workload_name": args.workload, **fn()}))
@@ -760,7 +807,7 @@ def main(argv=None):
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")
     ap.add_argument("--workload", default=None,
                     choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "widened",
-                             "pointwise", "served_mixed", "autotune_L24"],
+                             "pointwise", "expand", "served_mixed", "autotune_L24"],
                     help="run only this secondary workload and print its result")
     args = ap.parse_args(argv)
     set_polys(args.polys)
