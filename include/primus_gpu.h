@@ -408,6 +408,25 @@ int pg_glwe_encryptor_destroy(pg_glwe_encryptor *encryptor);
 int pg_glwe_encrypt(const pg_glwe_encryptor *encryptor, uint32_t k, const uint64_t *d_sk_ntt,
                     const uint64_t *d_msg, const uint64_t *h_scale, uint64_t seed, uint64_t stream0,
                     uint64_t *d_ct, size_t batch, void *stream);
+/* Public-key encryption (primus_fhe_core/src/public_key/glwe.rs).  A public key
+ * [k+1][L][N] (NTT domain) is a secret-key encryption of zero
+ * (DcrtGlwePublicKey::new, :33-71): pg_glwe_encrypt with d_msg = NULL.
+ * pg_glwe_pk_encrypt: DcrtGlwePublicKey::encrypt (:74-126) of `batch`
+ * ciphertexts, ct_c = NTT(e_c) + NTT(v) pk_c with scale_l * msg added to the
+ * body's noise before its NTT; samplers, for ciphertext j:
+ *   v   ternary: bits 2(x mod 16) of hash(seed, stream0 + 2^33 + j, x / 16):
+ *       0,1 -> 0, 2 -> 1, 3 -> -1
+ *   e_c discrete Gaussian (as pg_glwe_encrypt), stream stream0 + 2^32 + j (k+1) + c
+ * pg_ggsw_pk_encrypt_monomial: DcrtGlwePublicKey::encrypt_monomial_ggsw_inplace
+ * (:214-263), GGSW [k+1][d][k+1][L][N] of coeff * X^degree (degree < N): row
+ * r = i d + j is ciphertext r of the samplers above, with coeff_l * g_{j,l}
+ * added at coefficient `degree` of component i (:128-193). */
+int pg_glwe_pk_encrypt(const pg_glwe_encryptor *encryptor, uint32_t k, const uint64_t *d_pk,
+                       const uint64_t *d_msg, const uint64_t *h_scale, uint64_t seed, uint64_t stream0,
+                       uint64_t *d_ct, size_t batch, void *stream);
+int pg_ggsw_pk_encrypt_monomial(const pg_glwe_encryptor *encryptor, const pg_gadget_basis *basis, uint32_t k,
+                                const uint64_t *d_pk, const uint64_t *h_coeff_residues, size_t degree,
+                                uint64_t seed, uint64_t stream0, uint64_t *d_ggsw, void *stream);
 
 /* pg_ext_product for callers that cannot allocate device memory when they
  * call (hosts holding only device pointers owned by another runtime, serving

@@ -129,6 +129,10 @@ def lib():
             "orc_ntt_auto_perm": (None, [C.c_uint32, C.c_uint64, u32p]),
             "orc_glwe_automorphism": (None, [C.c_void_p, C.c_uint32, C.c_uint64, u64p, u64p, u64p]),
             "orc_glwe_trace": (None, [C.c_void_p, C.c_uint32, u64p, C.c_int, u64p, u64p]),
+            "orc_glwe_pk_encrypt_cdt": (None, [C.c_void_p, C.c_uint32, u64p, u64p, u64p, C.c_double, C.c_uint64,
+                                                C.c_uint64, C.c_uint64, u64p]),
+            "orc_ggsw_pk_encrypt_monomial": (None, [C.c_void_p, C.c_uint32, u64p, u64p, C.c_size_t, C.c_double,
+                                                     C.c_uint64, C.c_uint64, u64p]),
             "orc_glwe_expand": (None, [C.c_void_p, C.c_uint32, u64p, C.c_size_t, u64p, u64p]),
             "orc_cdt_table": (C.c_uint32, [C.c_double, u64p, C.c_uint32]),
             "orc_cdt_sample": (C.c_int64, [u64p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
@@ -523,6 +527,21 @@ class Lattice:
         lib().orc_glwe_encrypt_cdt(self.pctx, k, p64(u64(sk_ntt)), mp, p64(u64(scale)), sigma, seed, stream0, index,
                                    p64(ct))
         return ct
+
+    def pk_encrypt_cdt(self, k, pk, msg, scale, seed, stream0, index, sigma=3.2):
+        """DcrtGlwePublicKey::encrypt of ciphertext `index` with the counter-based samplers."""
+        ct = np.zeros((k + 1) * self.L * self.n, np.uint64)
+        mp = p64(u64(msg)) if msg is not None else None
+        sp = p64(u64(scale)) if scale is not None else None
+        lib().orc_glwe_pk_encrypt_cdt(self.pctx, k, p64(u64(pk)), mp, sp, sigma, seed, stream0, index, p64(ct))
+        return ct
+
+    def ggsw_pk_encrypt_monomial(self, k, pk, coeff_res, degree, seed, stream0, sigma=3.2):
+        """DcrtGlwePublicKey::encrypt_monomial_ggsw: [k+1][d][k+1][L][N]."""
+        out = np.zeros((k + 1) * self.d * (k + 1) * self.L * self.n, np.uint64)
+        lib().orc_ggsw_pk_encrypt_monomial(self.pctx, k, p64(u64(pk)), p64(u64(coeff_res)), degree, sigma, seed,
+                                           stream0, p64(out))
+        return out
 
     def ternary(self, seed, stream):
         out = np.zeros(self.L * self.n, np.uint64)

@@ -1701,3 +1701,73 @@ void orc_glwe_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *
                                c->tables[l]->q);
     }
 }
+
+/* one public-key encryption: DcrtGlwePublicKey::encrypt
+ * (primus_fhe_core/src/public_key/glwe.rs:74-126) with the counter-based
+ * samplers: v ternary (stream stream0 + 2^33 + index), e_c discrete Gaussian
+ * (stream stream0 + 2^32 + index (k+1) + c); ct_c = NTT(e_c + [c == mc] m_c) + v pk_c.
+ * The message enters component mc: a scaled polynomial (GLWE, mc = k) or one
+ * coefficient coeff_l * g_l at `degree` (a GGSW row, :128-193). */
+static void pk_encrypt_one(const orc_lattice_ctx *c, uint32_t k, const uint64_t *pk, const uint64_t *cdt,
+                           uint32_t entries, uint64_t seed, uint64_t stream0, uint64_t index, uint32_t mc,
+                           const uint64_t *msg, const uint64_t *scale, const uint64_t *mono_coeff,
+                           const uint64_t *mono_scalar, size_t degree, uint64_t *ct) {
+    const size_t n = c->n;
+    const uint32_t L = c->L;
+    const size_t poly = (size_t)L * n;
+    uint64_t *v = malloc(poly * 8), *moduli = malloc((size_t)L * 8);
+    for (uint32_t l = 0; l < L; ++l) moduli[l] = c->tables[l]->q;
+    orc_sample_ternary(seed, stream0 + (1ull << 33) + index, moduli, L, n, v);
+    for (uint32_t l = 0; l < L; ++l) orc_ntt_forward(c->tables[l], v + (size_t)l * n);
+    for (uint32_t comp = 0; comp <= k; ++comp) {
+        uint64_t *e = ct + (size_t)comp * poly;
+        for (size_t x = 0; x < n; ++x) {
+            const int64_t g = orc_cdt_sample(cdt, entries, seed, stream0 + (1ull << 32) + index * (k + 1) + comp, x);
+            for (uint32_t l = 0; l < L; ++l) {
+                const uint64_t q = moduli[l];
+                e[(size_t)l * n + x] = g >= 0 ? (uint64_t)g % q : q - (uint64_t)(-g) % q;
+            }
+        }
+        for (uint32_t l = 0; l < L; ++l) {
+            const uint64_t q = moduli[l];
+            if (comp == mc && msg) orc_add_mul_scalar_assign(e + (size_t)l * n, msg + (size_t)l * n, scale[l], n, q);
+            if (comp == mc && mono_coeff) {
+                uint64_t ratio[2];
+                orc_barrett_ratio(q, ratio);
+                e[(size_t)l * n + degree] =
+                    orc_barrett_reduce_mul_add(mono_coeff[l], mono_scalar[l], e[(size_t)l * n + degree], q, ratio);
+            }
+            orc_ntt_forward(c->tables[l], e + (size_t)l * n);
+            orc_add_mul_assign(e + (size_t)l * n, v + (size_t)l * n, pk + (size_t)comp * poly + (size_t)l * n, n, q);
+        }
+    }
+    free(v);
+    free(moduli);
+}
+
+void orc_glwe_pk_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *pk, const uint64_t *msg,
+                             const uint64_t *scale, double sigma, uint64_t seed, uint64_t stream0, uint64_t index,
+                             uint64_t *ct) {
+    uint64_t cdt[512];
+    const uint32_t entries = orc_cdt_table(sigma, cdt, 512);
+    pk_encrypt_one(c, k, pk, cdt, entries, seed, stream0, index, k, msg, scale, NULL, NULL, 0, ct);
+}
+
+/* DcrtGlwePublicKey::encrypt_monomial_ggsw_inplace (public_key/glwe.rs:214-263):
+ * row r = i d + j (GLev i = 0..k, digit j) is a public-key encryption whose
+ * component i carries coeff_l * g_{j,l} at `degree` (:128-193). */
+void orc_ggsw_pk_encrypt_monomial(const orc_lattice_ctx *c, uint32_t k, const uint64_t *pk,
+                                  const uint64_t *coeff_res, size_t degree, double sigma, uint64_t seed,
+                                  uint64_t stream0, uint64_t *ggsw) {
+    uint64_t cdt[512];
+    const uint32_t entries = orc_cdt_table(sigma, cdt, 512);
+    const uint32_t d = c->basis->decompose_length, L = c->L;
+    const size_t glwe = (size_t)(k + 1) * L * c->n;
+    const uint64_t *g = c->basis->scalar_residues; /* [d][L] */
+    for (uint32_t i = 0; i <= k; ++i)
+        for (uint32_t j = 0; j < d; ++j) {
+            const uint64_t r = (uint64_t)i * d + j;
+            pk_encrypt_one(c, k, pk, cdt, entries, seed, stream0, r, i, NULL, NULL, coeff_res, g + (size_t)j * L,
+                           degree, ggsw + r * glwe);
+        }
+}

@@ -322,6 +322,19 @@ int64_t orc_cdt_sample(const uint64_t *cdt, uint32_t entries, uint64_t seed, uin
 void orc_glwe_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *sk_ntt, const uint64_t *msg,
                           const uint64_t *scale, double sigma, uint64_t seed, uint64_t stream0, uint64_t index,
                           uint64_t *ct);
+/* public-key encryption (DcrtGlwePublicKey::encrypt, primus_fhe_core/src/public_key/glwe.rs:74-126)
+ * of ciphertext `index`: v ternary (stream stream0 + 2^33 + index), e_c CDT
+ * Gaussian (stream stream0 + 2^32 + index (k+1) + c), ct_c = NTT(e_c) + v pk_c,
+ * the body with scale_l * msg added before its NTT.  pk: [k+1][L][N] NTT domain
+ * (a secret-key encryption of zero, DcrtGlwePublicKey::new :33-71). */
+void orc_glwe_pk_encrypt_cdt(const orc_lattice_ctx *c, uint32_t k, const uint64_t *pk, const uint64_t *msg,
+                             const uint64_t *scale, double sigma, uint64_t seed, uint64_t stream0, uint64_t index,
+                             uint64_t *ct);
+/* DcrtGlwePublicKey::encrypt_monomial_ggsw_inplace (:214-263): GGSW [k+1][d][k+1][L][N]
+ * of coeff * X^degree; row r = i d + j uses index r of the samplers above. */
+void orc_ggsw_pk_encrypt_monomial(const orc_lattice_ctx *c, uint32_t k, const uint64_t *pk,
+                                  const uint64_t *coeff_res, size_t degree, double sigma, uint64_t seed,
+                                  uint64_t stream0, uint64_t *ggsw);
 
 /* ---- HEXL-style AVX-512 IFMA52 transforms (hexl_ifma.c): the reference's fastest
  * CPU path, timed as the CPU baseline (q < 2^50, n >= 16, host with avx512ifma) */

@@ -275,6 +275,24 @@ class GlweEncryptor:
         call("pg_glwe_encrypt", self.h, k, sk_ntt.ptr, msg.ptr if msg is not None else None, ptr(sc), seed, stream0,
              ct.ptr, batch, _sh(stream))
 
+    def public_key(self, k: int, sk_ntt: DeviceBuffer, seed: int, stream0: int, pk: DeviceBuffer, stream=None):
+        """DcrtGlwePublicKey::new: a secret-key encryption of zero, [k+1][L][N]."""
+        self.encrypt(k, sk_ntt, None, None, seed, stream0, pk, 1, stream=stream)
+
+    def pk_encrypt(self, k: int, pk: DeviceBuffer, msg: DeviceBuffer | None, scale, seed: int, stream0: int,
+                   ct: DeviceBuffer, batch: int, stream=None):
+        """DcrtGlwePublicKey::encrypt of `batch` ciphertexts."""
+        sc = np.ascontiguousarray(np.asarray(scale if scale is not None else [0] * self.table.L, dtype=np.uint64))
+        call("pg_glwe_pk_encrypt", self.h, k, pk.ptr, msg.ptr if msg is not None else None, ptr(sc), seed, stream0,
+             ct.ptr, batch, _sh(stream))
+
+    def ggsw_pk_encrypt_monomial(self, basis: GadgetBasis, k: int, pk: DeviceBuffer, coeff_residues, degree: int,
+                                 seed: int, stream0: int, ggsw: DeviceBuffer, stream=None):
+        """DcrtGlwePublicKey::encrypt_monomial_ggsw_inplace: [k+1][d][k+1][L][N]."""
+        cr = np.ascontiguousarray(np.asarray(coeff_residues, dtype=np.uint64))
+        call("pg_ggsw_pk_encrypt_monomial", self.h, basis.h, k, pk.ptr, ptr(cr), degree, seed, stream0, ggsw.ptr,
+             _sh(stream))
+
     def close(self):
         if getattr(self, "h", None):
             nat.lib().pg_glwe_encryptor_destroy(self.h)

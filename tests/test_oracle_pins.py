@@ -224,6 +224,30 @@ def test_external_product_decrypts(k):
         assert np.array_equal(lat.decrypt(k, sk_ntt, out, t, gamma), exp.astype(np.uint64))
 
 
+@pytest.mark.parametrize("k", [1, 2])
+def test_public_key_ggsw_external_product_decrypts(k):
+    # primus_fhe_core/tests/ext_prod.rs:58-113: the GGSW of X^degree is encrypted
+    # under the public key (DcrtGlwePublicKey::encrypt_monomial_ggsw), and a
+    # public-key GLWE encryption decrypts to its message
+    moduli = [1125899906826241, 1125899906629633]
+    table, base, basis, lat = _bfv_setup(k, 9, moduli, 30)
+    t, gamma = 12289, 2199023190017
+    sk = np.concatenate([lat.ternary(31, 10 + i) for i in range(k)])
+    sk_ntt = table.forward(sk)
+    pk = lat.encrypt_cdt(k, sk_ntt, None, [0, 0], 0x9C, 0, 0)
+    delta = lat.delta(t)
+    for trial, degree in enumerate([0, 101, 511]):
+        msg_small = O.uniform(200 + trial, 1, t, 512)
+        msg = base.wrapping_decompose_small(msg_small, t)
+        ct = lat.pk_encrypt_cdt(k, pk, msg, delta, 0x9D, 0, trial)
+        assert np.array_equal(lat.decrypt(k, sk_ntt, ct, t, gamma), msg_small)
+        ggsw = lat.ggsw_pk_encrypt_monomial(k, pk, [1, 1], degree, 0x9E, (1 << 20) + 100 * trial)
+        out = lat.external_product(k, table.inverse(ct), ggsw)
+        exp = np.roll(msg_small.astype(np.int64), degree)
+        exp[:degree] = (t - exp[:degree]) % t
+        assert np.array_equal(lat.decrypt(k, sk_ntt, out, t, gamma), exp.astype(np.uint64))
+
+
 def test_key_switch_decrypts():
     # primus_fhe_core/tests/ksk.rs: dimension 3, N = 512, log_basis 20
     moduli = [1125899906826241, 1125899906629633]
