@@ -476,6 +476,10 @@ static void free_table(pg_ntt_table* t) {
     cudaFree(t->d_inv_n);
     cudaFree(t->d_inv_last);
     cudaFree(t->d_barrett);
+    cudaFree(t->d_fwd_fp);
+    cudaFree(t->d_inv_fp);
+    cudaFree(t->d_inv_n_fp);
+    cudaFree(t->d_inv_last_fp);
     delete t;
 }
 
@@ -533,6 +537,41 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
     if (e == cudaSuccess)
         e = cudaMemcpy(t->d_inv_last, invlast.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->d_barrett, bar.data(), L * sizeof(Barrett), cudaMemcpyHostToDevice);
+    // FP64-schedule copies: (w, w / q) as doubles (exact values, correctly rounded quotients)
+    uint64_t maxq = 0;
+    for (uint64_t m : t->moduli) maxq = m > maxq ? m : maxq;
+    if (e == cudaSuccess && maxq < (1ull << 50)) {
+        auto fp = [](const ulonglong2& v, uint64_t q) {
+            const double w = (double)v.x;
+            const double wq = w / (double)q;
+            uint64_t a, b;
+            std::memcpy(&a, &w, 8);
+            std::memcpy(&b, &wq, 8);
+            return make_ulonglong2(a, b);
+        };
+        std::vector<ulonglong2> ffwd(L * n), finv(L * n), finvn(L), finvlast(L);
+        for (size_t l = 0; l < L; ++l) {
+            const uint64_t q = t->moduli[l];
+            for (size_t i = 0; i < n; ++i) {
+                ffwd[l * n + i] = fp(fwd[l * n + i], q);
+                finv[l * n + i] = fp(inv[l * n + i], q);
+            }
+            finvn[l] = fp(invn[l], q);
+            finvlast[l] = fp(invlast[l], q);
+        }
+        e = cudaMalloc(&t->d_fwd_fp, L * n * sizeof(ulonglong2));
+        if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_fp, L * n * sizeof(ulonglong2));
+        if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_n_fp, L * sizeof(ulonglong2));
+        if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_last_fp, L * sizeof(ulonglong2));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(t->d_fwd_fp, ffwd.data(), L * n * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(t->d_inv_fp, finv.data(), L * n * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(t->d_inv_n_fp, finvn.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(t->d_inv_last_fp, finvlast.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         free_table(t);
         return cuda_status(e, "pg_ntt_table_create: device upload");

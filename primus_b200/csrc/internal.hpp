@@ -96,6 +96,12 @@ struct pg_ntt_table {
     ulonglong2* d_inv_n = nullptr;     // [L] N^-1
     ulonglong2* d_inv_last = nullptr;  // [L] inv_root_powers[N-1] * N^-1
     pg::Barrett* d_barrett = nullptr;  // [L]
+    // the four twiddle tables above with (w, w / q) as doubles, for the FP64
+    // schedule; allocated when every modulus is below 2^50
+    ulonglong2* d_fwd_fp = nullptr;
+    ulonglong2* d_inv_fp = nullptr;
+    ulonglong2* d_inv_n_fp = nullptr;
+    ulonglong2* d_inv_last_fp = nullptr;
     int variant[3] = {0, 0, 0};        // NTT kernel shape per mode (forward, inverse, round trip)
 };
 
@@ -121,6 +127,11 @@ struct NttArgs {
     const uint64_t* plain;
     const uint64_t* plain_q;
     const Barrett* bar;
+    // FP64-schedule twiddles: the same tables with (w, w / q) as doubles
+    const ulonglong2* fwd_fp;
+    const ulonglong2* inv_fp;
+    const ulonglong2* inv_n_fp;
+    const ulonglong2* inv_last_fp;
     const RowDesc* desc;  // NULL: rows are [polys][L][N] at data
     uint64_t rows;
     uint64_t max_modulus;
@@ -164,6 +175,10 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     a.plain = nullptr;
     a.plain_q = nullptr;
     a.bar = t->d_barrett;
+    a.fwd_fp = t->d_fwd_fp;
+    a.inv_fp = t->d_inv_fp;
+    a.inv_n_fp = t->d_inv_n_fp;
+    a.inv_last_fp = t->d_inv_last_fp;
     a.desc = nullptr;
     a.rows = rows;
     a.max_modulus = 0;
@@ -179,6 +194,7 @@ int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
 // of the canonical forward, the inverse and the round trip; identical results
 int ntt_variant_count(uint32_t log_n);
 const char* ntt_variant_name(uint32_t log_n, int variant);
+bool ntt_variant_fp(uint32_t log_n, int variant);  // FP64 schedule: every q < 2^50
 int launch_ntt_variant(const NttArgs& a, uint32_t log_n, int mode, int variant, cudaStream_t stream);
 
 // hybrid key switch context accessors (Q limb count, ring degree)

@@ -253,18 +253,26 @@ int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
     if (a.rows == 0) return PG_OK;
     const bool ffwd = fast_fwd_ok(a), finv = fast_inv_ok(a);
     // a tuned shape runs the fast schedules: canonical forward, inverse and round trip
-    if (mode >= 0 && mode < 3 && a.variant[mode] > 0 &&
-        (mode == MODE_FWD ? (!a.lazy && ffwd) : finv))
-        return launch_ntt_variant(a, log_n, mode, a.variant[mode], st);
+    if (mode >= 0 && mode < 3 && a.variant[mode] > 0) {
+        const bool ok = ntt_variant_fp(log_n, a.variant[mode])
+                            ? finv && a.fwd_fp && (mode != MODE_FWD || !a.lazy)
+                            : (mode == MODE_FWD ? (!a.lazy && ffwd) : finv);
+        if (ok) return launch_ntt_variant(a, log_n, mode, a.variant[mode], st);
+    }
+    // the FP64 schedule (every q < 2^50, tables present) is the fastest on every shape
+    const bool ffp = finv && a.fwd_fp;
     switch (mode) {
         case MODE_FWD:
+            if (!a.lazy && ffp) return launch_mode<MODE_FWD, kSchedFp64>(a, log_n, st);
             if (!a.lazy && ffwd) return launch_mode<MODE_FWD, kSchedFastFwd>(a, log_n, st);
             return launch_mode<MODE_FWD, kSchedExact>(a, log_n, st);
         case MODE_INV:
             // the inverse's outputs are canonical on every schedule (lazy included)
+            if (ffp) return launch_mode<MODE_INV, kSchedFp64>(a, log_n, st);
             if (finv) return launch_mode<MODE_INV, kSchedFastBoth>(a, log_n, st);
             return launch_mode<MODE_INV, kSchedExact>(a, log_n, st);
         case MODE_RT:
+            if (ffp) return launch_mode<MODE_RT, kSchedFp64>(a, log_n, st);
             if (finv) return launch_mode<MODE_RT, kSchedFastBoth>(a, log_n, st);
             if (ffwd) return launch_mode<MODE_RT, kSchedFastFwd>(a, log_n, st);
             return launch_mode<MODE_RT, kSchedExact>(a, log_n, st);

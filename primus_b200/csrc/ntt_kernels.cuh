@@ -127,6 +127,80 @@ PG_DEV uint64_t canon4(uint64_t v, uint64_t q, uint64_t q2) {
     return v >= q ? v - q : v;
 }
 
+// ---------------------------------------------------------------------------
+// FP64 schedule (kSchedFp64, every q < 2^50).  The B200 FP64 pipe issues as
+// many operations per clock as the integer multiply pipe and is idle in the
+// integer schedules, and a double holds every integer below 2^53 exactly, so
+// residues travel as doubles holding signed integers and every operation
+// below is exact (each result is an integer of magnitude below 2^53, which
+// round-to-nearest reproduces).  Register and shared-memory words keep the
+// double's bit pattern.  Twiddle tables hold (w, wq) with wq = w / q
+// correctly rounded (wq < 1 because w < q).
+//
+// fmulmod(y, w, wq, q) = w y mod q in (-0.75 q, 0.75 q) for |y| < 2^51:
+//   t  = fma(y, wq, 1.5*2^52) rounds y*wq to the nearest integer (|y wq| < 2^51
+//        keeps t in [2^52, 2^53), where doubles are the integers), qt = t - 1.5*2^52;
+//        |qt - y w/q| <= 1/2 + |y| 2^-53 < 3/4.
+//   ph = fl(qt q), pl = qt q - ph exactly (the error of a product, by fma);
+//        |qt| < 2^51 so |ph| < 2^101 and |pl| <= 2^47.
+//   r  = fma(w, y, -ph) = (w y - qt q) + pl exactly: |w y - qt q| < 0.75 q and
+//        |pl| <= 2^47, so the exact value is an integer below 2^53.
+//   r - pl = w y - qt q, exact.
+// freduce(x, q, qinv) = x - rint(x qinv) q in [-q/2 - 1, q/2 + 1] for |x| < 2^53.
+// ---------------------------------------------------------------------------
+constexpr double kMagic52 = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double kTwo52 = 4503599627370496.0;    // 2^52
+
+PG_DEV double as_f(uint64_t b) { return __longlong_as_double((long long)b); }
+PG_DEV uint64_t as_u(double d) { return (uint64_t)__double_as_longlong(d); }
+// exact conversions of integers in [0, 2^52)
+PG_DEV double u52_to_f(uint64_t v) { return __dsub_rn(as_f(v | 0x4330000000000000ull), kTwo52); }
+PG_DEV uint64_t f_to_u52(double d) { return as_u(__dadd_rn(d, kTwo52)) & 0xFFFFFFFFFFFFFull; }
+
+PG_DEV double fmulmod(double y, double w, double wq, double q) {
+    const double qt = __dsub_rn(__fma_rn(y, wq, kMagic52), kMagic52);
+    const double ph = __dmul_rn(qt, q);
+    const double pl = __fma_rn(qt, q, -ph);
+    const double r = __fma_rn(w, y, -ph);
+    return __dsub_rn(r, pl);
+}
+
+PG_DEV double freduce(double x, double q, double qinv) {
+    const double qt = __dsub_rn(__fma_rn(x, qinv, kMagic52), kMagic52);
+    return __fma_rn(-qt, q, x);
+}
+
+// x in (-q, q) -> [0, q)
+PG_DEV double fcanon(double x, double q) { return x < 0.0 ? __dadd_rn(x, q) : x; }
+
+// Cooley-Tukey forward butterfly: (u + w y, u - w y).  RU reduces u first.
+// Inputs below 2q + 2 in magnitude; with u reduced at least every other stage
+// (the stages of even bit index p) the outputs stay below 2q + 2: a reducing
+// stage gives at most q/2 + 1 + 0.75 q, the next one adds at most 0.75 q.
+template <bool RU>
+PG_DEV void fwd_bfly_fp(uint64_t& x, uint64_t& y, const ulonglong2 w, double q, double qinv) {
+    double u = as_f(x);
+    if constexpr (RU) u = freduce(u, q, qinv);
+    const double v = fmulmod(as_f(y), as_f(w.x), as_f(w.y), q);
+    x = as_u(__dadd_rn(u, v));
+    y = as_u(__dsub_rn(u, v));
+}
+
+// Gentleman-Sande inverse butterfly: (reduce(u + v), w (u - v)); inputs below
+// q in magnitude (u - v below 2q < 2^51), outputs below 0.75 q.
+PG_DEV void inv_bfly_fp(uint64_t& x, uint64_t& y, const ulonglong2 w, double q, double qinv) {
+    const double u = as_f(x), v = as_f(y);
+    x = as_u(freduce(__dadd_rn(u, v), q, qinv));
+    y = as_u(fmulmod(__dsub_rn(u, v), as_f(w.x), as_f(w.y), q));
+}
+
+// last inverse stage fused with N^-1; writes canonical integers (not doubles)
+PG_DEV void inv_last_bfly_fp(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, double q) {
+    const double u = as_f(x), v = as_f(y);
+    x = f_to_u52(fcanon(fmulmod(__dadd_rn(u, v), as_f(s.x), as_f(s.y), q), q));
+    y = f_to_u52(fcanon(fmulmod(__dsub_rn(u, v), as_f(sr.x), as_f(sr.y), q), q));
+}
+
 // insert LOG_E zero bits at bit position g into t
 template <int LOG_E>
 PG_DEV uint32_t group_base(uint32_t t, int g) {
@@ -148,7 +222,9 @@ PG_DEV void ldg_tw2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
 // sp = LOG_M-1-p and uses tw[(tw_base << sp) + (i >> (p+1))], tw_base = C + rank
 // for a cluster block (1 for a whole row).  When a stage needs two or more
 // twiddles their first index is even, so they are fetched in 32-byte pairs.
-template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, bool FAST>
+// K: 0 = exact schedule, 1 = fast integer schedule, 2 = FP64 schedule (then q2
+// and nq carry the bit patterns of q and 1/q as doubles and tw is the FP64 table)
+template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, int K>
 PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
                       uint64_t q2, uint64_t nq) {
     constexpr int E = 1 << LOG_E;
@@ -163,7 +239,9 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
             constexpr int k = decltype(kk)::value;
             static_for<0, half>([&](auto ll) {
                 constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
-                if constexpr (FAST)
+                if constexpr (K == 2)
+                    fwd_bfly_fp<(p & 1) == 0>(x[jj], x[jj + half], w, as_f(q2), as_f(nq));
+                else if constexpr (K == 1)
                     fwd_bfly_fast(x[jj], x[jj + half], w, q2, nq);
                 else
                     fwd_bfly(x[jj], x[jj + half], w, q2, nq);
@@ -196,10 +274,15 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // from the earliest start that round can have, kFastInvReduceStage - LOG_E + 1
 // (a bound at least as large as the true one).  Outputs are canonical either
 // way, so the values equal the exact Harvey schedule's.
-template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, bool FASTI = false>
+//
+// KI: 0 = exact, 1 = the unreduced integer schedule above (FASTI), 2 = FP64
+// schedule (q and nq carry the bit patterns of q and 1/q as doubles, the
+// tables are the FP64 ones; the last stage writes canonical integers).
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, int KI = 0>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
                       const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq,
                       uint64_t inv64 = 0) {
+    constexpr bool FASTI = KI == 1, FP = KI == 2;
     const uint64_t q2 = 2 * q;
     constexpr int E = 1 << LOG_E;
     constexpr uint32_t N = 1u << LOG_N;
@@ -221,7 +304,12 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
             const ulonglong2 s = *sptr, sr = *srptr;
             static_for<0, E>([&](auto jt) {
                 constexpr int jj = decltype(jt)::value;
-                if constexpr (!(jj & half)) inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq, bnd);
+                if constexpr (!(jj & half)) {
+                    if constexpr (FP)
+                        inv_last_bfly_fp(x[jj], x[jj + half], s, sr, as_f(q));
+                    else
+                        inv_last_bfly(x[jj], x[jj + half], s, sr, q, nq, bnd);
+                }
             });
         } else {
             const ulonglong2* row = itw + (N - (N >> p)) + (((rank << LOG_M) + base) >> (p + 1));
@@ -229,7 +317,9 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
                 constexpr int k = decltype(kk)::value;
                 static_for<0, half>([&](auto ll) {
                     constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
-                    if constexpr (FASTI)
+                    if constexpr (FP)
+                        inv_bfly_fp(x[jj], x[jj + half], w, as_f(q), as_f(nq));
+                    else if constexpr (FASTI)
                         inv_bfly_fast(x[jj], x[jj + half], w, bnd, nq);
                     else
                         inv_bfly(x[jj], x[jj + half], w, q2, nq);
@@ -280,7 +370,7 @@ struct FwdRounds {
 // Runs forward rounds R..last; x holds round R-1's group on entry (stored to
 // smem first).  On exit x holds the last round's group (G = 0: E contiguous
 // elements at tid*E).
-template <int LOG_M, int TOP, int LOG_E, int R, bool FAST>
+template <int LOG_M, int TOP, int LOG_E, int R, int FAST>
 PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
                      const ulonglong2* __restrict__ tw, uint64_t q2, uint64_t nq) {
     if constexpr (R < FwdRounds<TOP, LOG_E, 0>::COUNT) {
@@ -306,7 +396,7 @@ struct InvRounds {
 
 // Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
 // (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
-template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END, bool FASTI = false>
+template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END, int FASTI = 0>
 PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
                       const ulonglong2* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
                       uint64_t nq, uint64_t inv64 = 0) {
@@ -323,6 +413,27 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
     }
 }
 
+// Butterfly schedules (template parameter S of the kernels).  All return the same
+// canonical values; the faster ones need headroom below 2^64 (or 2^53):
+//   kSchedExact    the reference's Harvey / Gentleman-Sande schedule (lazy outputs)
+//   kSchedFastFwd  forward without the u = x mod 2q step: every q < 2^58
+//   kSchedFastBoth also the inverse without the x reduction: every q < 2^50
+//   kSchedFp64     both directions on the FP64 pipe (fwd_bfly_fp / inv_bfly_fp):
+//                  every q < 2^50, canonical (non-lazy) forward outputs
+constexpr int kSchedExact = 0, kSchedFastFwd = 1, kSchedFastBoth = 2, kSchedFp64 = 3;
+
+// per-row constants of the FP64 schedule: q and 1/q (correctly rounded)
+struct FpMod {
+    double q, qinv;
+};
+
+PG_DEV FpMod fp_mod(uint64_t qi) {
+    FpMod m;
+    m.q = u52_to_f(qi);
+    m.qinv = __drcp_rn(m.q);
+    return m;
+}
+
 // ============================================================================
 // Single-CTA kernel: ROWS rows of N = 2^LOG_N per CTA, T = N/E threads per row.
 // FAST selects the forward schedule without per-butterfly reduction of u (only
@@ -331,7 +442,9 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
 template <int LOG_N, int LOG_E, int ROWS, int MODE, int S>
 __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kernel(NttArgs a) {
     constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E;
-    constexpr bool FAST = S >= 1, FASTI = S >= 2;  // schedules: see kSched* below
+    constexpr bool FP = S == kSchedFp64;
+    constexpr int KF = FP ? 2 : (S >= 1 ? 1 : 0), KI = FP ? 2 : (S >= 2 ? 1 : 0);  // round kinds
+    constexpr bool FAST = KF == 1, FASTI = KI == 1;
     extern __shared__ uint64_t smem_block[];
     const uint32_t tid = threadIdx.x;
     // launch order is limb-major (all polys of limb 0, then limb 1, ...) so that
@@ -351,19 +464,28 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
         mulp = d.mul;
     }
     const uint64_t q = a.moduli[limb], q2 = q << 1, nq = 0 - q;
+    const FpMod fm = fp_mod(FP ? q : 3);
+    // the rounds' modulus words: (2q, -q) on the integer schedules, (q, 1/q) as doubles on FP64
+    const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
     uint64_t x[E];
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
-        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        const ulonglong2* tw = (FP ? a.fwd_fp : a.fwd) + (size_t)limb * N;
         using R0 = FwdRounds<LOG_N, LOG_E, 0>;
         // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
 #pragma unroll
-        for (int jj = 0; jj < E; ++jj) x[jj] = active ? g[tid + jj * T] : 0;
-        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, tw, q2, nq);
-        fwd_rest<LOG_N, LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, tw, q2, nq);
+        for (int jj = 0; jj < E; ++jj) {
+            x[jj] = active ? g[tid + jj * T] : 0;
+            if constexpr (FP) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
+        }
+        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, KF>(x, tid, 1, tw, mA, mB);
+        fwd_rest<LOG_N, LOG_N, LOG_E, 1, KF>(x, sm, tid, 1, tw, mA, mB);
         // x = E contiguous outputs at tid*E
         if constexpr (MODE == MODE_FWD) {
-            if constexpr (FAST) {
+            if constexpr (FP) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = f_to_u52(fcanon(freduce(as_f(x[jj]), fm.q, fm.qinv), fm.q));
+            } else if constexpr (FAST) {
                 const uint64_t inv64 = a.bar[limb].r1;
 #pragma unroll
                 for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
@@ -383,15 +505,26 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             // the lazy product in [0, 2q) is a valid inverse input
             const uint64_t* pv = a.plain + (size_t)limb * N + tid * E;
             const uint64_t* pq = a.plain_q + (size_t)limb * N + tid * E;
+            if constexpr (FP) {
+                // w = plaintext (canonical), wq = w * (1/q): within 2^-52 relative of w/q, so the
+                // product of |x| < 2q + 2 lands in [-q, q] (a valid inverse input)
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+                for (int jj = 0; jj < E; ++jj) {
+                    const double w = u52_to_f(__ldg(pv + jj));
+                    x[jj] = as_u(fmulmod(as_f(x[jj]), w, __dmul_rn(w, fm.qinv), fm.q));
+                }
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+            }
         }
     }
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
-        const ulonglong2* itw = a.inv + (size_t)limb * N;
-        const ulonglong2* sptr = a.inv_n + limb;
-        const ulonglong2* srptr = a.inv_last + limb;
+        const ulonglong2* itw = (FP ? a.inv_fp : a.inv) + (size_t)limb * N;
+        const ulonglong2* sptr = (FP ? a.inv_n_fp : a.inv_n) + limb;
+        const ulonglong2* srptr = (FP ? a.inv_last_fp : a.inv_last) + limb;
+        const uint64_t iA = FP ? as_u(fm.q) : q, iB = FP ? as_u(fm.qinv) : nq;
         using I0 = InvRounds<LOG_N, LOG_E, 0>;
         if constexpr (MODE == MODE_INV) {
             // stage the bit-reversed row through smem (coalesced), then round 0
@@ -400,6 +533,7 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
                 uint64_t v = active ? g[tid + k * T] : 0;
                 // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
                 if (mulp && active) v = barrett_mul(v, mulp[tid + k * T], a.bar[limb]);
+                if constexpr (FP) v = as_u(freduce(u52_to_f(v), fm.q, fm.qinv));  // inputs < 2q < 2^52
                 sm[padi(tid + k * T)] = v;
             }
             __syncthreads();
@@ -410,9 +544,9 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             static_assert(I0::G == 0, "round trip needs the first inverse group to be contiguous");
         }
         const uint64_t inv64 = FASTI ? a.bar[limb].r1 : 0;
-        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI, FASTI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr,
-                                                                         srptr, q, nq, inv64);
-        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT, FASTI>(x, sm, tid, 0, itw, sptr, srptr, q, nq, inv64);
+        inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI, KI>(x, group_base<LOG_E>(tid, I0::G), 0, itw, sptr,
+                                                                      srptr, iA, iB, inv64);
+        inv_range<LOG_N, LOG_N, LOG_N, LOG_E, 1, I0::COUNT, KI>(x, sm, tid, 0, itw, sptr, srptr, iA, iB, inv64);
         // last group: elements tid + jj*T, coalesced store
         using Last = InvRounds<LOG_N, LOG_E, I0::COUNT - 1>;
         static_assert(Last::G == LOG_N - LOG_E, "last inverse group");
@@ -455,7 +589,9 @@ __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 
 template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
 __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
     ntt_cluster_kernel(NttArgs a) {
-    constexpr bool FAST = S >= 1, FASTI = S >= 2;  // schedules: see kSched* below
+    constexpr bool FP = S == kSchedFp64;
+    constexpr int KF = FP ? 2 : (S >= 1 ? 1 : 0), KI = FP ? 2 : (S >= 2 ? 1 : 0);  // round kinds
+    constexpr bool FAST = KF == 1, FASTI = KI == 1;
     constexpr int LOG_C = LOG_N - LOG_M;
     constexpr int N = 1 << LOG_N, M = 1 << LOG_M, E = 1 << LOG_E, LOG_T = LOG_M - LOG_E, T = 1 << LOG_T;
     constexpr int LOG_K = LOG_E - LOG_C;  // top block bits handled by the cross phase
@@ -482,18 +618,24 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         mulp = d.mul;
     }
     const uint64_t q = a.moduli[limb], nq = 0 - q;
+    const FpMod fm = fp_mod(FP ? q : 3);
     const uint32_t gt = (rank << LOG_T) + tid;  // cross group (column) of this thread
     uint64_t x[E];
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
         const uint64_t q2 = q << 1;
-        const ulonglong2* tw = a.fwd + (size_t)limb * N;
+        // the rounds' modulus words: (2q, -q) on the integer schedules, (q, 1/q) as doubles on FP64
+        const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
+        const ulonglong2* tw = (FP ? a.fwd_fp : a.fwd) + (size_t)limb * N;
         // matched by the wait before the first remote store; relaxed is enough
         // because this CTA has not touched shared memory yet
         cluster_arrive_relaxed();
 #pragma unroll
-        for (int jj = 0; jj < E; ++jj) x[jj] = g[gt + (jj << GX)];
-        fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, FAST>(x, gt, 1, tw, q2, nq);
+        for (int jj = 0; jj < E; ++jj) {
+            x[jj] = g[gt + (jj << GX)];
+            if constexpr (FP) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
+        }
+        fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, KF>(x, gt, 1, tw, mA, mB);
         cluster_wait_acquire();  // every CTA of the cluster is running
         // element gt + jj*N/E lives in block jj >> LOG_K at local index gt + (jj & (K-1)) * N/E
         const uint32_t la = smem_u32(sm + padi(gt));
@@ -505,11 +647,14 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         // local rounds over the low TOP block bits
         using R0 = FwdRounds<TOP, LOG_E, 0>;
         load_smem<LOG_E, R0::G>(x, sm, group_base<LOG_E>(tid, R0::G));
-        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, group_base<LOG_E>(tid, R0::G), (1u << LOG_C) + rank,
-                                                                 tw, q2, nq);
-        fwd_rest<LOG_M, TOP, LOG_E, 1, FAST>(x, sm, tid, (1u << LOG_C) + rank, tw, q2, nq);
+        fwd_round<LOG_M, LOG_E, R0::G, R0::P_HI, R0::P_LO, KF>(x, group_base<LOG_E>(tid, R0::G), (1u << LOG_C) + rank,
+                                                               tw, mA, mB);
+        fwd_rest<LOG_M, TOP, LOG_E, 1, KF>(x, sm, tid, (1u << LOG_C) + rank, tw, mA, mB);
         if constexpr (MODE == MODE_FWD) {
-            if constexpr (FAST) {
+            if constexpr (FP) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = f_to_u52(fcanon(freduce(as_f(x[jj]), fm.q, fm.qinv), fm.q));
+            } else if constexpr (FAST) {
                 const uint64_t inv64 = a.bar[limb].r1;
 #pragma unroll
                 for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
@@ -526,13 +671,23 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         } else {
             const uint64_t* pv = a.plain + (size_t)limb * N + rank * M + tid * E;
             const uint64_t* pq = a.plain_q + (size_t)limb * N + rank * M + tid * E;
+            if constexpr (FP) {
+                // as in the block kernel: products in [-q, q]
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+                for (int jj = 0; jj < E; ++jj) {
+                    const double w = u52_to_f(__ldg(pv + jj));
+                    x[jj] = as_u(fmulmod(as_f(x[jj]), w, __dmul_rn(w, fm.qinv), fm.q));
+                }
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) x[jj] = shoup_lazy_nq(__ldg(pv + jj), __ldg(pq + jj), x[jj], nq);
+            }
         }
     }
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
-        const ulonglong2* itw = a.inv + (size_t)limb * N;
+        const ulonglong2* itw = (FP ? a.inv_fp : a.inv) + (size_t)limb * N;
+        const uint64_t iA = FP ? as_u(fm.q) : q, iB = FP ? as_u(fm.qinv) : nq;
         using I0 = InvRounds<TOP, LOG_E, 0>;
         using ILast = InvRounds<TOP, LOG_E, I0::COUNT - 1>;
         static_assert(I0::COUNT >= 2, "cluster path needs two local rounds");
@@ -543,16 +698,17 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
                 uint64_t v = gb[tid + k * T];
                 // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
                 if (mulp) v = barrett_mul(v, mulp[rank * M + tid + k * T], a.bar[limb]);
+                if constexpr (FP) v = as_u(freduce(u52_to_f(v), fm.q, fm.qinv));  // inputs < 2q < 2^52
                 sm[padi(tid + k * T)] = v;
             }
             __syncthreads();
             load_smem<LOG_E, I0::G>(x, sm, group_base<LOG_E>(tid, I0::G));
         }
         const uint64_t inv64 = FASTI ? a.bar[limb].r1 : 0;
-        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI, FASTI>(x, group_base<LOG_E>(tid, I0::G), rank, itw,
-                                                                         nullptr, nullptr, q, nq, inv64);
-        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1, FASTI>(x, sm, tid, rank, itw, nullptr, nullptr, q, nq,
-                                                                     inv64);
+        inv_round<LOG_N, LOG_M, LOG_E, I0::G, I0::P_LO, I0::P_HI, KI>(x, group_base<LOG_E>(tid, I0::G), rank, itw,
+                                                                      nullptr, nullptr, iA, iB, inv64);
+        inv_range<LOG_N, LOG_M, TOP, LOG_E, 1, I0::COUNT - 1, KI>(x, sm, tid, rank, itw, nullptr, nullptr, iA, iB,
+                                                                  inv64);
         {
             // last local round: its smem loads precede the cluster arrive, so no
             // CTA overwrites a block that another CTA is still reading
@@ -564,8 +720,8 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
             // release: these shared-memory reads must be performed before any
             // other CTA, released by this barrier, overwrites the block
             cluster_arrive_release();
-            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI, FASTI>(x, base, rank, itw, nullptr,
-                                                                                      nullptr, q, nq, inv64);
+            inv_round<LOG_N, LOG_M, LOG_E, ILast::G, ILast::P_LO, ILast::P_HI, KI>(x, base, rank, itw, nullptr,
+                                                                                   nullptr, iA, iB, inv64);
             cluster_wait_acquire();
             // element at row index i = rank*M + base + (jj << G) belongs to cross
             // group c = i mod N/E (CTA c >> LOG_T, thread c mod T) as element i >> GX:
@@ -583,8 +739,8 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         // cross inverse stages (the last LOG_E, including the N^-1-scaled one)
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = sm[padi((jj << LOG_T) + tid)];
-        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1, FASTI>(x, gt, 0, itw, a.inv_n + limb, a.inv_last + limb, q,
-                                                                 nq, inv64);
+        inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1, KI>(x, gt, 0, itw, (FP ? a.inv_n_fp : a.inv_n) + limb,
+                                                              (FP ? a.inv_last_fp : a.inv_last) + limb, iA, iB, inv64);
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
     }
@@ -594,12 +750,6 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
 
 namespace pg {
 
-// Butterfly schedules (template parameter S of the kernels).  All return the same
-// canonical values; the faster ones need headroom below 2^64:
-//   kSchedExact    the reference's Harvey / Gentleman-Sande schedule (lazy outputs)
-//   kSchedFastFwd  forward without the u = x mod 2q step: every q < 2^58
-//   kSchedFastBoth also the inverse without the x reduction: every q < 2^50
-constexpr int kSchedExact = 0, kSchedFastFwd = 1, kSchedFastBoth = 2;
 inline bool fast_fwd_ok(const NttArgs& a) { return a.max_modulus < (1ull << 58); }
 inline bool fast_inv_ok(const NttArgs& a) { return a.max_modulus < (1ull << 50); }
 

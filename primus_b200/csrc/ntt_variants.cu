@@ -21,27 +21,37 @@ struct VariantInfo {
     uint32_t log_n;
     int variant;
     const char* name;
+    bool fp;  // FP64 schedule: every q < 2^50, canonical outputs
 };
 
 // variant 0 is the default of each degree (ntt.cu); these are 1, 2, ...
 constexpr VariantInfo kVariants[] = {
-    {10, 1, "block E=8, 2 rows per CTA"},        {10, 2, "block E=4, 256 threads"},
-    {11, 1, "block E=16, 128 threads"},          {11, 2, "block E=16, 2 rows per CTA"},
-    {12, 1, "block E=8, 512 threads"},           {12, 2, "block E=16, 2 rows per CTA"},
-    {12, 3, "cluster of 2 x 2048"},
-    {13, 1, "block E=8, 1024 threads"},          {13, 2, "block E=16, 512 threads"},
-    {13, 3, "cluster of 4 x 2048"},
-    {14, 1, "cluster of 2 x 8192"},              {14, 2, "block E=16, 1024 threads"},
-    {14, 3, "cluster of 8 x 2048"},
-    {15, 1, "cluster of 4 x 8192"},              {15, 2, "cluster of 16 x 2048"},
-    {16, 1, "cluster of 8 x 8192"},
+    {10, 1, "block E=8, 2 rows per CTA", false},  {10, 2, "block E=4, 256 threads", false},
+    {10, 3, "fp64 block E=8", true},              {10, 4, "fp64 block E=8, 2 rows per CTA", true},
+    {11, 1, "block E=16, 128 threads", false},    {11, 2, "block E=16, 2 rows per CTA", false},
+    {11, 3, "fp64 block E=8", true},              {11, 4, "fp64 block E=16, 128 threads", true},
+    {12, 1, "block E=8, 512 threads", false},     {12, 2, "block E=16, 2 rows per CTA", false},
+    {12, 3, "cluster of 2 x 2048", false},        {12, 4, "fp64 block E=16", true},
+    {12, 5, "fp64 cluster of 2 x 2048", true},
+    {13, 1, "block E=8, 1024 threads", false},    {13, 2, "block E=16, 512 threads", false},
+    {13, 3, "cluster of 4 x 2048", false},        {13, 4, "fp64 cluster of 2 x 4096", true},
+    {13, 5, "fp64 cluster of 4 x 2048", true},
+    {14, 1, "cluster of 2 x 8192", false},        {14, 2, "block E=16, 1024 threads", false},
+    {14, 3, "cluster of 8 x 2048", false},        {14, 4, "fp64 cluster of 4 x 4096", true},
+    {14, 5, "fp64 cluster of 2 x 8192", true},
+    {15, 1, "cluster of 4 x 8192", false},        {15, 2, "cluster of 16 x 2048", false},
+    {15, 3, "fp64 cluster of 8 x 4096", true},    {15, 4, "fp64 cluster of 4 x 8192", true},
+    {16, 1, "cluster of 8 x 8192", false},        {16, 2, "fp64 cluster of 16 x 4096", true},
+    {16, 3, "fp64 cluster of 8 x 8192", true},
 };
 
 template <int MODE>
 int run_variant(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
-    // the variants run the fast schedules: the forward every q < 2^58, the
-    // inverse and the round trip every q < 2^50 (canonical outputs)
+    // the integer variants run the fast schedules: the forward every q < 2^58,
+    // the inverse and the round trip every q < 2^50 (canonical outputs); the
+    // FP64 variants every q < 2^50
     constexpr int F = MODE == MODE_FWD ? kSchedFastFwd : kSchedFastBoth;
+    constexpr int D = kSchedFp64;
     switch (log_n * 8 + (uint32_t)v) {
         case 10 * 8 + 1: return launch_block<10, 3, 2, MODE, F>(a, st);
         case 10 * 8 + 2: return launch_block<10, 2, 1, MODE, F>(a, st);
@@ -59,6 +69,20 @@ int run_variant(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
         case 15 * 8 + 1: return launch_cluster<15, 13, 4, MODE, F>(a, st);
         case 15 * 8 + 2: return launch_cluster<15, 11, 4, MODE, F>(a, st);
         case 16 * 8 + 1: return launch_cluster<16, 13, 4, MODE, F>(a, st);
+        case 10 * 8 + 3: return launch_block<10, 3, 1, MODE, D>(a, st);
+        case 10 * 8 + 4: return launch_block<10, 3, 2, MODE, D>(a, st);
+        case 11 * 8 + 3: return launch_block<11, 3, 1, MODE, D>(a, st);
+        case 11 * 8 + 4: return launch_block<11, 4, 1, MODE, D>(a, st);
+        case 12 * 8 + 4: return launch_block<12, 4, 1, MODE, D>(a, st);
+        case 12 * 8 + 5: return launch_cluster<12, 11, 4, MODE, D>(a, st);
+        case 13 * 8 + 4: return launch_cluster<13, 12, 4, MODE, D>(a, st);
+        case 13 * 8 + 5: return launch_cluster<13, 11, 4, MODE, D>(a, st);
+        case 14 * 8 + 4: return launch_cluster<14, 12, 4, MODE, D>(a, st);
+        case 14 * 8 + 5: return launch_cluster<14, 13, 4, MODE, D>(a, st);
+        case 15 * 8 + 3: return launch_cluster<15, 12, 4, MODE, D>(a, st);
+        case 15 * 8 + 4: return launch_cluster<15, 13, 4, MODE, D>(a, st);
+        case 16 * 8 + 2: return launch_cluster<16, 12, 4, MODE, D>(a, st);
+        case 16 * 8 + 3: return launch_cluster<16, 13, 4, MODE, D>(a, st);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
 }
@@ -70,6 +94,12 @@ int ntt_variant_count(uint32_t log_n) {
     for (const auto& v : kVariants)
         if (v.log_n == log_n) ++c;
     return c;
+}
+
+bool ntt_variant_fp(uint32_t log_n, int variant) {
+    for (const auto& v : kVariants)
+        if (v.log_n == log_n && v.variant == variant) return v.fp;
+    return false;
 }
 
 const char* ntt_variant_name(uint32_t log_n, int variant) {
@@ -180,9 +210,10 @@ int pg_ntt_autotune(pg_ntt_table* t, size_t polys, pg_ntt_tuning* out) {
     for (int mode = 0; mode < 3; ++mode) {
         int best = 0;
         float best_us = 0;
-        // alternative shapes exist on the fast schedules only
-        const int vmax = (mode == MODE_FWD ? ffwd : finv) ? count : 1;
-        for (int v = 0; v < vmax; ++v) {
+        for (int v = 0; v < count; ++v) {
+            // alternative shapes exist on the fast schedules only (FP64: every q < 2^50)
+            if (v > 0 && !(ntt_variant_fp(t->log_n, v) ? finv && a.fwd_fp : (mode == MODE_FWD ? ffwd : finv)))
+                continue;
             float us = 0;
             rc = time_variant(a, t->log_n, mode, v, b.st, b.e0, b.e1, &us);
             if (rc) return rc;
