@@ -261,8 +261,12 @@ def run_gpu(args):
     # table before the warm-up and keeps the fastest in the table
     tuning = tab.autotune(POLYS)
     rt_shape = tuning["round_trip"]
-    kernel_name = ("ntt_cluster_kernel<16,12,4,RT,fast>" if rt_shape["variant"] == 0
-                   else "ntt_cluster_kernel<16,13,4,RT,fast>")
+    # template arguments <LOG_N, LOG_M (block), LOG_E, MODE (2 = round trip), schedule>;
+    # schedule 3 = FP64 butterflies (every q < 2^50, the default there), 2 = fast integer
+    kernel_name = {"default": "ntt_cluster_kernel<16, 12, 4, 2, 3>",
+                   "fp64 cluster of 16 x 4096": "ntt_cluster_kernel<16, 12, 4, 2, 3>",
+                   "fp64 cluster of 8 x 8192": "ntt_cluster_kernel<16, 13, 4, 2, 3>",
+                   "cluster of 8 x 8192": "ntt_cluster_kernel<16, 13, 4, 2, 2>"}.get(rt_shape["name"], rt_shape["name"])
 
     def step():
         tab.polymul_ntt_plain(data, plain, plain_q, POLYS, stream=stream)
