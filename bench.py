@@ -375,7 +375,10 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,
                          "kernel": kernel_name + " (fused fwd -> x plain -> inv)",
-                         "algorithmic_bytes_per_launch": ALGO_BYTES},
+                         "algorithmic_bytes_per_launch": ALGO_BYTES,
+                         # the bound that binds: arithmetic issue (FP64 pipe on the FP64 schedule)
+                         "butterflies_per_launch": NTT_PER_STEP * L * (N // 2) * LOG_N,
+                         "g_butterflies_per_s": NTT_PER_STEP * L * (N // 2) * LOG_N / (per_step / 1e3) / 1e9},
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
             "cpu_baseline": cpu,
