@@ -336,6 +336,28 @@ def run_gpu(args):
     nat.call("pg_host_free", hp.value)
     e2e_value = NTT_PER_STEP * world / (e2e_ms / 1e3)
 
+    # ---- the same fused step on the integer schedules only (FP64 schedule off):
+    # identical residues, the butterflies on the integer multiply pipe
+    integer_only = None
+    if tab.fp64:
+        tab.set_fp64(False)
+        int_tuning = tab.autotune(POLYS)
+        for _ in range(3):
+            step()
+        stream.synchronize()
+        int_steps = max(3, args.steps // 2)
+        e0.record(stream)
+        for _ in range(int_steps):
+            step()
+        e1.record(stream)
+        stream.synchronize()
+        int_ms = e0.elapsed_ms(e1) / int_steps
+        tab.set_fp64(True)
+        integer_only = {"value": NTT_PER_STEP / (int_ms / 1e3), "unit": UNIT, "ms_per_step": int_ms,
+                        "kernel_shape": int_tuning["round_trip"]["name"],
+                        "note": "pg_ntt_set_fp64(table, 0): the same fused step with integer butterflies "
+                                "(Shoup products on the integer multiply pipe); same outputs"}
+
     peak, peak_kind = load_peaks()
     achieved = ALGO_BYTES / (per_step / 1e3) / 1e9
     out = None
@@ -379,6 +401,7 @@ def run_gpu(args):
                          # the bound that binds: arithmetic issue (FP64 pipe on the FP64 schedule)
                          "butterflies_per_launch": NTT_PER_STEP * L * (N // 2) * LOG_N,
                          "g_butterflies_per_s": NTT_PER_STEP * L * (N // 2) * LOG_N / (per_step / 1e3) / 1e9},
+            "integer_only": integer_only,
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
             "cpu_baseline": cpu,

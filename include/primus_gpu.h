@@ -134,6 +134,15 @@ int pg_ntt_autotune(pg_ntt_table *table, size_t polys, pg_ntt_tuning *out);
 int pg_ntt_variant_count(uint32_t log_n);
 const char *pg_ntt_variant_name(uint32_t log_n, int variant); /* NULL if out of range */
 int pg_ntt_set_variant(pg_ntt_table *table, int mode, int variant);
+/* FP64 butterfly schedule on (enable = 1, the default when every modulus is
+ * below 2^50) or off (0: every transform of this table runs on the integer
+ * pipe only).  Both schedules return the same canonical residues: the FP64 one
+ * carries residues as doubles holding integers below 2^53, each operation's
+ * result exact (quotient estimates are corrected exactly, as Shoup's are).
+ * No reference counterpart.  Returns PG_ERR_UNSUPPORTED when enabling it on a
+ * table with a modulus at or above 2^50.  Resets the autotuned shapes. */
+int pg_ntt_set_fp64(pg_ntt_table *table, int enable);
+int pg_ntt_fp64_enabled(const pg_ntt_table *table);
 /* poly_length(), moduli_count(), crt_poly_length() */
 int pg_ntt_table_info(const pg_ntt_table *table, uint32_t *log_n, uint32_t *moduli_count,
                       size_t *poly_length, size_t *crt_poly_length);

@@ -571,6 +571,7 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
             e = cudaMemcpy(t->d_inv_n_fp, finvn.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
             e = cudaMemcpy(t->d_inv_last_fp, finvlast.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+        t->fp64 = e == cudaSuccess;
     }
     if (e != cudaSuccess) {
         free_table(t);
@@ -579,6 +580,17 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
     *out = t;
     return PG_OK;
 }
+
+int pg_ntt_set_fp64(pg_ntt_table* t, int enable) {
+    if (!t) return set_error(PG_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (enable && !t->d_fwd_fp)
+        return set_error(PG_ERR_UNSUPPORTED, "the FP64 schedule needs every modulus below 2^50");
+    t->fp64 = enable ? 1 : 0;
+    for (int m = 0; m < 3; ++m) t->variant[m] = 0;  // tuned shapes belong to the previous schedule
+    return PG_OK;
+}
+
+int pg_ntt_fp64_enabled(const pg_ntt_table* t) { return t && t->fp64 ? 1 : 0; }
 
 int pg_ntt_table_destroy(pg_ntt_table* table) {
     free_table(table);

@@ -239,6 +239,7 @@ void make_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_tab
     v.d_inv_n = t->d_inv_n + first;
     v.d_inv_last = t->d_inv_last + first;
     v.d_barrett = t->d_barrett + first;
+    v.fp64 = t->fp64;
     if (t->d_fwd_fp) {  // FP64 tables (every modulus below 2^50)
         v.d_fwd_fp = t->d_fwd_fp + (size_t)first * t->n;
         v.d_inv_fp = t->d_inv_fp + (size_t)first * t->n;

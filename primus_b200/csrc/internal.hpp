@@ -102,6 +102,7 @@ struct pg_ntt_table {
     ulonglong2* d_inv_fp = nullptr;
     ulonglong2* d_inv_n_fp = nullptr;
     ulonglong2* d_inv_last_fp = nullptr;
+    int fp64 = 0;                       // FP64 schedule in use (tables present and not switched off)
     int variant[3] = {0, 0, 0};        // NTT kernel shape per mode (forward, inverse, round trip)
 };
 
@@ -175,7 +176,7 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     a.plain = nullptr;
     a.plain_q = nullptr;
     a.bar = t->d_barrett;
-    a.fwd_fp = t->d_fwd_fp;
+    a.fwd_fp = t->fp64 ? t->d_fwd_fp : nullptr;  // null: integer schedules only
     a.inv_fp = t->d_inv_fp;
     a.inv_n_fp = t->d_inv_n_fp;
     a.inv_last_fp = t->d_inv_last_fp;

@@ -198,6 +198,15 @@ class DcrtTable:
         """Force kernel shape `variant` for mode 0 (canonical forward), 1 (inverse) or 2 (round trip)."""
         call("pg_ntt_set_variant", self.h, mode, variant)
 
+    def set_fp64(self, enable: bool):
+        """Switch the FP64 butterfly schedule on or off (pg_ntt_set_fp64); off keeps every
+        transform on the integer pipe.  Same results either way."""
+        call("pg_ntt_set_fp64", self.h, int(bool(enable)))
+
+    @property
+    def fp64(self) -> bool:
+        return bool(nat.lib().pg_ntt_fp64_enabled(self.h))
+
     # ---- pointwise (device)
     def mul(self, x, y, polys, rhs_polys=None, stream=None):
         call("pg_dcrt_mul", self.h, x.ptr, y.ptr, polys, polys if rhs_polys is None else rhs_polys, _sh(stream))

@@ -133,3 +133,34 @@ def test_fp64_shapes_skip_wide_moduli(gpu):
         assert np.array_equal(d.numpy(), ref.forward(x.copy()))
         t.inverse(d, 1)
         assert np.array_equal(d.numpy(), x)
+
+
+def test_fp64_switch_keeps_values(gpu):
+    """pg_ntt_set_fp64: integer-only and FP64 schedules give the same residues; the
+    switch is refused for a modulus at or above 2^50."""
+    P = gpu
+    log_n, n, L, polys = 14, 1 << 14, 3, 2
+    moduli = O.ntt_primes(1 << 50, 2 * n, L)
+    t = P.DcrtTable(log_n, moduli)
+    assert t.fp64
+    ref = O.DcrtTable(log_n, moduli)
+    x = np.concatenate([O.uniform_rns(0xE1, 10 * p, moduli, n).ravel() for p in range(polys)])
+    plain = O.uniform_rns(0xE2, 0, moduli, n)
+    dplain = P.DeviceBuffer.from_numpy(plain)
+    dq = P.DeviceBuffer(plain.size)
+    t.shoup_prepare(dplain, dq, 1)
+    for fp in (False, True, False):
+        t.set_fp64(fp)
+        assert t.fp64 == fp
+        d = P.DeviceBuffer.from_numpy(x)
+        t.forward(d, polys)
+        assert np.array_equal(d.numpy(), ref.forward(x.copy()))
+        t.inverse(d, polys)
+        assert np.array_equal(d.numpy(), x)
+        d = P.DeviceBuffer.from_numpy(x)
+        t.polymul_ntt_plain(d, dplain, dq, polys)
+        assert np.array_equal(d.numpy(), ref.polymul_roundtrip(x.copy(), plain))
+    wide = P.DcrtTable(12, O.ntt_primes(1 << 55, 2 << 12, 1))
+    assert not wide.fp64
+    with pytest.raises(P.PrimusGpuError):
+        wide.set_fp64(True)
