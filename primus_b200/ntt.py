@@ -270,10 +270,18 @@ class PolymulBatch:
         call("pg_polymul_batch_create", arr, len(self.tables), C.byref(h))
         self.h = h.value
 
+    @staticmethod
+    def prepare(jobs):
+        """The C job array for `jobs` ((a, b, log_n, moduli_count) tuples), built once:
+        a caller that resubmits the same job set passes it to run() and skips the
+        per-call Python conversion (what a C or Rust caller holds anyway)."""
+        return (PolymulJob * len(jobs))(*[PolymulJob(a.ptr, b.ptr, ln, L) for a, b, ln, L in jobs])
+
     def run(self, jobs, use_graph=True, stream=None):
-        """jobs: iterable of (a: DeviceBuffer, b: DeviceBuffer, log_n, moduli_count)."""
-        arr = (PolymulJob * len(jobs))(*[PolymulJob(a.ptr, b.ptr, ln, L) for a, b, ln, L in jobs])
-        call("pg_polymul_batch_run", self.h, arr, len(jobs), int(bool(use_graph)), _sh(stream))
+        """jobs: iterable of (a: DeviceBuffer, b: DeviceBuffer, log_n, moduli_count), or
+        the array prepare() returned."""
+        arr = jobs if isinstance(jobs, C.Array) else self.prepare(jobs)
+        call("pg_polymul_batch_run", self.h, arr, len(arr), int(bool(use_graph)), _sh(stream))
 
     def close(self):
         if getattr(self, "h", None):
