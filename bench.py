@@ -731,7 +731,8 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
             a, b = P.DeviceBuffer(t.L << ln), P.DeviceBuffer(t.L << ln)
             t.fill_uniform(a, 1, seed=seed + 3, stream0=64 * i, stream=stream)
             t.fill_uniform(b, 1, seed=seed + 4, stream0=64 * i, stream=stream)
-            trace.append(("pm", a, b, ln, L))
+            # the job array is built once, as the served request is
+            trace.append(("pm", a, b, ln, L, pm_batch.prepare([(a, b, ln, L)])))
         elif kd == 1:
             di, do = P.DeviceBuffer(2 * 2048), P.DeviceBuffer(2 * 2048)
             xt.fill_uniform(di, 2, seed=seed + 5, stream0=2 * i, stream=stream)
@@ -745,7 +746,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     # ---- plain: one synchronous call per request, in arrival order
     def plain_call(it):
         if it[0] == "pm":
-            pm_batch.run([(it[1], it[2], it[3], it[4])], use_graph=False, stream=stream)
+            pm_batch.run(it[5], use_graph=False, stream=stream)
         elif it[0] == "xp":
             P.external_product(xt, xg, 1, it[1], xkey, it[2], 1, stream=stream)
         else:
