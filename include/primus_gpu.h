@@ -119,8 +119,9 @@ int pg_ntt_table_destroy(pg_ntt_table *table);
  * every shape of the table's degree on `polys` seeded polys of its moduli (at
  * most 1 GiB) for the canonical forward, the inverse and the fused round trip,
  * and keeps the fastest of each in the table.  The alternatives run on the fast
- * schedules only (canonical forward: every modulus below 2^58; inverse and
- * round trip: below 2^50); the lazy forward always runs the default shape.  It allocates its own buffers and synchronizes; call it before
+ * schedules only (integer shapes: canonical forward with every modulus below
+ * 2^58, inverse and round trip below 2^50; FP64 shapes: every modulus below 2^50
+ * and the FP64 schedule enabled); the lazy forward always runs the default shape.  It allocates its own buffers and synchronizes; call it before
  * the table is shared between threads or streams.  No reference counterpart
  * (the reference's CPU transforms have one shape). */
 typedef struct pg_ntt_tuning {
