@@ -141,7 +141,8 @@ int pg_ntt_set_variant(pg_ntt_table *table, int mode, int variant);
  * carries residues as doubles holding integers below 2^53, each operation's
  * result exact (quotient estimates are corrected exactly, as Shoup's are).
  * No reference counterpart.  Returns PG_ERR_UNSUPPORTED when enabling it on a
- * table with a modulus at or above 2^50.  Resets the autotuned shapes. */
+ * table with a modulus at or above 2^50.  Resets the autotuned shapes; like
+ * pg_ntt_autotune, call it before the table is shared between threads or streams. */
 int pg_ntt_set_fp64(pg_ntt_table *table, int enable);
 int pg_ntt_fp64_enabled(const pg_ntt_table *table);
 /* poly_length(), moduli_count(), crt_poly_length() */
