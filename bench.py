@@ -261,6 +261,8 @@ def run_gpu(args):
     # table before the warm-up and keeps the fastest in the table
     tuning = tab.autotune(POLYS)
     rt_shape = tuning["round_trip"]
+    # built-in ceilings (streaming copy, register-only butterfly rates), measured before the warm-up
+    cal = P.calibrate()
     # template arguments <LOG_N, LOG_M (block), LOG_E, MODE (2 = round trip), schedule>;
     # schedule 3 = FP64 butterflies (every q < 2^50, the default there), 2 = fast integer
     kernel_name = {"default": "ntt_cluster_kernel<16, 12, 4, 2, 3>",
@@ -353,7 +355,10 @@ def run_gpu(args):
         stream.synchronize()
         int_ms = e0.elapsed_ms(e1) / int_steps
         tab.set_fp64(True)
+        int_gbfly = NTT_PER_STEP * L * (N // 2) * LOG_N / (int_ms / 1e3) / 1e9
         integer_only = {"value": NTT_PER_STEP / (int_ms / 1e3), "unit": UNIT, "ms_per_step": int_ms,
+                        "g_butterflies_per_s": int_gbfly,
+                        "frac_of_int_ceiling": int_gbfly / cal["int_butterflies_gps"],
                         "kernel_shape": int_tuning["round_trip"]["name"],
                         "note": "pg_ntt_set_fp64(table, 0): the same fused step with integer butterflies "
                                 "(Shoup products on the integer multiply pipe); same outputs"}
@@ -400,7 +405,14 @@ def run_gpu(args):
                          "algorithmic_bytes_per_launch": ALGO_BYTES,
                          # the bound that binds: arithmetic issue (FP64 pipe on the FP64 schedule)
                          "butterflies_per_launch": NTT_PER_STEP * L * (N // 2) * LOG_N,
-                         "g_butterflies_per_s": NTT_PER_STEP * L * (N // 2) * LOG_N / (per_step / 1e3) / 1e9},
+                         "g_butterflies_per_s": NTT_PER_STEP * L * (N // 2) * LOG_N / (per_step / 1e3) / 1e9,
+                         "compute_ceiling": {
+                             "pipe": "fp64" if tab.fp64 else "integer",
+                             "g_butterflies_per_s": cal["fp64_butterflies_gps" if tab.fp64 else "int_butterflies_gps"],
+                             "frac": (NTT_PER_STEP * L * (N // 2) * LOG_N / (per_step / 1e3) / 1e9)
+                                     / cal["fp64_butterflies_gps" if tab.fp64 else "int_butterflies_gps"],
+                             "source": "pg_calibrate: register-only forward butterflies of the same schedule"},
+                         "builtin_copy_gbs": cal["hbm_copy_gbs"]},
             "integer_only": integer_only,
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},

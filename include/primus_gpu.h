@@ -132,6 +132,17 @@ typedef struct pg_ntt_tuning {
 } pg_ntt_tuning;
 enum { PG_NTT_MODE_FORWARD = 0, PG_NTT_MODE_INVERSE = 1, PG_NTT_MODE_ROUND_TRIP = 2 };
 int pg_ntt_autotune(pg_ntt_table *table, size_t polys, pg_ntt_tuning *out);
+/* Built-in ceilings on the current device (no reference counterpart): a
+ * streaming copy of 512 MiB (read + write bytes per second, GB/s) and the
+ * register-only rate of the forward butterfly on the fast integer schedule and
+ * on the FP64 schedule (G butterflies/s, q just below 2^50).  Allocates 1 GiB
+ * and synchronizes the device; a measurement call, not for a serving path. */
+typedef struct pg_calibration {
+    double hbm_copy_gbs;
+    double int_butterflies_gps;
+    double fp64_butterflies_gps;
+} pg_calibration;
+int pg_calibrate(pg_calibration *out);
 int pg_ntt_variant_count(uint32_t log_n);
 const char *pg_ntt_variant_name(uint32_t log_n, int variant); /* NULL if out of range */
 int pg_ntt_set_variant(pg_ntt_table *table, int mode, int variant);

@@ -14,7 +14,7 @@ from .lattice import (BaseConverter, GadgetBasis, RnsBase, RnsError, external_pr
 from .server import (Request, Server, ext_product_request, key_switch_request,  # noqa: F401
                      polymul_request)
 from .ntt import (DcrtTable, NttError, NttTable, PolymulBatch, host_tables, minimal_primitive_root,  # noqa: F401
-                  ntt_primes, prev_prime_congruent, variant_count, variant_name)
+                  ntt_primes, prev_prime_congruent, variant_count, variant_name, calibrate)
 
 __all__ = [
     "DcrtTable", "NttTable", "NttError", "DeviceBuffer", "Stream", "Event", "PrimusGpuError",

@@ -74,6 +74,20 @@ def variant_name(log_n: int, variant: int) -> str:
     return r.decode() if r else ""
 
 
+class Calibration(C.Structure):
+    _fields_ = [("hbm_copy_gbs", C.c_double), ("int_butterflies_gps", C.c_double),
+                ("fp64_butterflies_gps", C.c_double)]
+
+
+def calibrate() -> dict:
+    """Built-in ceilings on the current device (pg_calibrate): streaming-copy GB/s and the
+    register-only forward-butterfly rate (G/s) on the integer and the FP64 schedule."""
+    c = Calibration()
+    call("pg_calibrate", C.byref(c))
+    return {"hbm_copy_gbs": c.hbm_copy_gbs, "int_butterflies_gps": c.int_butterflies_gps,
+            "fp64_butterflies_gps": c.fp64_butterflies_gps}
+
+
 class DcrtTable:
     """Device-resident NTT tables for L primes of degree N = 2^log_n
     (UintCrtNttTable, primus_ntt/src/dcrt/primitive.rs)."""

@@ -164,3 +164,11 @@ def test_fp64_switch_keeps_values(gpu):
     assert not wide.fp64
     with pytest.raises(P.PrimusGpuError):
         wide.set_fp64(True)
+
+
+def test_calibration_ceilings(gpu):
+    """pg_calibrate: the built-in ceilings are positive and in a sane range for a B200."""
+    c = gpu.calibrate()
+    assert 1000 < c["hbm_copy_gbs"] < 20000
+    assert 50 < c["int_butterflies_gps"] < 10000
+    assert 50 < c["fp64_butterflies_gps"] < 10000
