@@ -158,6 +158,14 @@ PG_DEV uint64_t barrett_reduce_shifted(uint64_t lo, uint64_t hi, const Barrett& 
     return r >= m.q ? r - m.q : r;
 }
 
+// any 128-bit x mod q: the shifted form (four multiplies) when x < 2^(n+62),
+// which holds for sums of up to 2^(62-n) products of residues, else the
+// 128-bit ratio form; the same canonical residue either way
+PG_DEV uint64_t barrett_reduce_128(uint64_t lo, uint64_t hi, const Barrett& m) {
+    if (m.mu && (hi >> (62 - __clzll(m.q))) == 0) return barrett_reduce_shifted(lo, hi, m);
+    return barrett_reduce_2limb(lo, hi, m);
+}
+
 PG_DEV uint64_t barrett_mul(uint64_t a, uint64_t b, const Barrett& m) {
     const uint64_t lo = a * b, hi = mulhi64(a, b);
     return m.mu ? barrett_reduce_shifted(lo, hi, m) : barrett_reduce_2limb(lo, hi, m);

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) phase_kernel(PhaseArgs a) {
             uint64_t lo = 0, hi = 0;
             for (uint32_t i = 0; i < a.k; ++i) {
                 if (i && (i & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
-                    lo = barrett_reduce_2limb(lo, hi, m);
+                    lo = barrett_reduce_128(lo, hi, m);
                     hi = 0;
                 }
                 const uint64_t x = ct[(size_t)i * LN + lx], s = a.sk[(size_t)i * LN + lx];
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(256) phase_kernel(PhaseArgs a) {
                 lo += pl;
                 hi += phi + (lo < pl);
             }
-            a.ph[b * LN + lx] = sub_mod(ct[(size_t)a.k * LN + lx], barrett_reduce_2limb(lo, hi, m), m.q);
+            a.ph[b * LN + lx] = sub_mod(ct[(size_t)a.k * LN + lx], barrett_reduce_128(lo, hi, m), m.q);
         }
     }
 }
@@ -83,9 +83,9 @@ __global__ void __launch_bounds__(256) convert_kernel(ConvertArgs a) {
             uint64_t lt = 0, ht = 0, lg = 0, hg = 0;
             for (uint32_t l = 0; l < a.L; ++l) {
                 if (l && (l & 7) == 0) {  // keep the sums below 2^128
-                    lt = barrett_reduce_2limb(lt, ht, a.bt);
+                    lt = barrett_reduce_128(lt, ht, a.bt);
                     ht = 0;
-                    lg = barrett_reduce_2limb(lg, hg, a.bg);
+                    lg = barrett_reduce_128(lg, hg, a.bg);
                     hg = 0;
                 }
                 const ulonglong2 f = a.scale[l];
@@ -99,8 +99,8 @@ __global__ void __launch_bounds__(256) convert_kernel(ConvertArgs a) {
                 lg += pl;
                 hg += phi + (lg < pl);
             }
-            const uint64_t yt = barrett_mul(barrett_reduce_2limb(lt, ht, a.bt), a.minus_inv_q_t, a.bt);
-            const uint64_t yg = barrett_mul(barrett_reduce_2limb(lg, hg, a.bg), a.minus_inv_q_g, a.bg);
+            const uint64_t yt = barrett_mul(barrett_reduce_128(lt, ht, a.bt), a.minus_inv_q_t, a.bt);
+            const uint64_t yg = barrett_mul(barrett_reduce_128(lg, hg, a.bg), a.minus_inv_q_g, a.bg);
             uint64_t temp = a.bg.q - yg + yt;
             if (temp >= a.bg.q) temp -= a.bg.q;
             a.msg[b * N + x] = shoup_mul(a.inv_gamma_t, a.inv_gamma_t_q, temp, a.bt.q);

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) mask_body_kernel(BodyArgs a) {
             uint64_t lo = 0, hi = 0;
             for (uint32_t i = 0; i < a.k; ++i) {
                 if (i && (i & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
-                    lo = barrett_reduce_2limb(lo, hi, m);
+                    lo = barrett_reduce_128(lo, hi, m);
                     hi = 0;
                 }
                 const uint64_t av = uniform_at(a.seed, a.stream0 + (j * a.k + i) * a.L + l, x, m.q);
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256) mask_body_kernel(BodyArgs a) {
                 lo += pl;
                 hi += ph + (lo < pl);
             }
-            ct[(size_t)a.k * LN + lx] = add_mod(a.eb[j * LN + lx], barrett_reduce_2limb(lo, hi, m), m.q);
+            ct[(size_t)a.k * LN + lx] = add_mod(a.eb[j * LN + lx], barrett_reduce_128(lo, hi, m), m.q);
         }
     }
 }

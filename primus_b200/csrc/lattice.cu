@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
                     for (uint32_t cc = 0; cc < kMacOut; ++cc)
 #pragma unroll
                         for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-                            lo[cc][bb] = barrett_reduce_2limb(lo[cc][bb], hi[cc][bb], m);
+                            lo[cc][bb] = barrett_reduce_128(lo[cc][bb], hi[cc][bb], m);
                             hi[cc][bb] = 0;
                         }
                 }
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
                     if (bb >= nb) break;
                     const size_t b = b0 + bb;
                     const size_t bc = b * a.KOUT + c;
-                    const uint64_t s = barrett_reduce_2limb(lo[cc][bb], hi[cc][bb], m);
+                    const uint64_t s = barrett_reduce_128(lo[cc][bb], hi[cc][bb], m);
                     uint64_t r;
                     if (a.negate) {
                         const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;

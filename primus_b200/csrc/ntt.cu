@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
                     for (int h = 0; h < 2; ++h) {
                         ulonglong2 s = acc[(c * E + e + h) * T + tid];
                         if (fold) {
-                            s.x = barrett_reduce_2limb(s.x, s.y, bar);
+                            s.x = barrett_reduce_128(s.x, s.y, bar);
                             s.y = 0;
                         }
                         const uint64_t kv = h ? w.y : w.x;
@@ -121,8 +121,8 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
 #pragma unroll
             for (int e = 0; e < E; e += 2) {
                 const ulonglong2 s0 = acc[(c * E + e) * T + tid], s1 = acc[(c * E + e + 1) * T + tid];
-                const uint64_t r0 = barrett_reduce_2limb(s0.x, s0.y, bar);
-                const uint64_t r1 = barrett_reduce_2limb(s1.x, s1.y, bar);
+                const uint64_t r0 = barrett_reduce_128(s0.x, s0.y, bar);
+                const uint64_t r1 = barrett_reduce_128(s1.x, s1.y, bar);
                 asm volatile("st.global.v2.u64 [%0], {%1, %2};" ::"l"(out + c * N + tid * E + e), "l"(r0), "l"(r1)
                              : "memory");
             }
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const ulonglong2 s = acc[(c * E + e) * T + tid];
-            x[e] = barrett_reduce_2limb(s.x, s.y, bar);
+            x[e] = barrett_reduce_128(s.x, s.y, bar);
         }
         __syncthreads();  // earlier shared-memory reads of the exchange buffer are done
         inv_round<LOG_N, LOG_N, LOG_E, I0::G, I0::P_LO, I0::P_HI>(x, tid * E, 0, a.inv, a.inv_n, a.inv_last, q, nq);

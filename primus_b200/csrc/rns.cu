@@ -280,11 +280,11 @@ __global__ void __launch_bounds__(256) fast_convert_kernel(const uint64_t* __res
             for (uint32_t i = 0; i < Li; ++i) {
                 mac128(lo, hi, buf[i], row[i]);
                 if ((i & 7) == 7) {  // keep the sum below 2^128 (terms < 2^124)
-                    lo = barrett_reduce_2limb(lo, hi, m);
+                    lo = barrett_reduce_128(lo, hi, m);
                     hi = 0;
                 }
             }
-            out[(size_t)j * n + x] = barrett_reduce_2limb(lo, hi, m);
+            out[(size_t)j * n + x] = barrett_reduce_128(lo, hi, m);
         }
     }
 }
