@@ -24,10 +24,11 @@
 // limbs -> pconv_kernel (P -> Q) -> forward NTT of the converted rows and of b
 // -> finish_kernel.  Each step runs over the whole batch in one launch.
 #include <algorithm>
+#include <cstring>
 #include <new>
 #include <vector>
 
-#include "internal.hpp"
+#include "ntt_kernels.cuh"
 
 using namespace pg;
 
@@ -48,6 +49,10 @@ struct pg_hybrid_ks {
     ulonglong2* d_pmat = nullptr;    // [L][K] Shoup pair of (P/p_k) mod q_l
     ulonglong2* d_pinv = nullptr;    // [L] Shoup pair of (P^-1 mod q_l)
     uint32_t* d_offs = nullptr;      // [2 * dnum]: gmat_off then gout_off
+    // FP64 copies for moduli below 2^50: (w, w / r) as doubles, and (q, 1/q) per limb
+    ulonglong2* d_gmat_fp = nullptr;
+    ulonglong2* d_pmat_fp = nullptr;
+    ulonglong2* d_fmod = nullptr;  // [L+K]
 };
 
 namespace {
@@ -65,6 +70,8 @@ struct ModUpArgs {
     uint64_t* ext;       // [B*k_in][dnum][L+K][N]
     const ulonglong2* ginv;
     const ulonglong2* gmat;
+    const ulonglong2* gmat_fp;  // FP64 form of gmat (FP kernels)
+    const ulonglong2* fmod;     // [L+K] (q, 1/q) as doubles (FP kernels)
     const uint32_t* gout;
     const uint32_t* gmat_off;  // [dnum]
     const uint32_t* gout_off;  // [dnum]
@@ -75,8 +82,10 @@ struct ModUpArgs {
 };
 
 // one thread per (input mask, group, coefficient); grid y = mask * dnum + group.
-// AMAX bounds the group size (registers held per thread).
-template <uint32_t AMAX>
+// AMAX bounds the group size (registers held per thread).  FP: the dot products
+// run on the FP64 pipe (fmulmod, every modulus below 2^50): each product lies in
+// (-0.75 r, 0.75 r), a sum of at most 8 below 6 r < 2^53, reduced exactly to [0, r).
+template <uint32_t AMAX, bool FP>
 __global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
     const uint32_t LK = a.L + a.K;
     const size_t outer = a.polys * a.dnum;
@@ -112,28 +121,55 @@ __global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
                     }
                 }
             }
-#pragma unroll 2
-            for (uint32_t j = 0; j < LK - ag; ++j) {
-                const uint32_t r = outl[j];
-                const uint64_t rq = a.moduli[r], nq = 0 - rq;
-                // sums of at most 8 lazy products in [0, 2 r): below 16 r < 2^64
-                uint64_t y0 = 0, y1 = 0;
+            if constexpr (FP) {
+                double td0[AMAX], td1[AMAX];
 #pragma unroll
-                for (uint32_t m = 0; m < AMAX; ++m)
-                    if (m < ag) {
-                        const ulonglong2 w = mat[j * ag + m];
-                        y0 += shoup_lazy_nq(w.x, w.y, tv0[m], nq);
-                        y1 += shoup_lazy_nq(w.x, w.y, tv1[m], nq);
-                    }
-                // [0, 4 r) is enough: the forward NTT that follows accepts inputs below
-                // 4q and returns canonical values of the same residues
-                if (AMAX > 4) {
-                    y0 = y0 >= 8 * rq ? y0 - 8 * rq : y0;
-                    y1 = y1 >= 8 * rq ? y1 - 8 * rq : y1;
+                for (uint32_t m = 0; m < AMAX; ++m) {
+                    td0[m] = u52_to_f(tv0[m]);
+                    td1[m] = u52_to_f(tv1[m]);
                 }
-                uint64_t* d = dst0 + (size_t)r * a.N;
-                d[x0] = y0 >= 4 * rq ? y0 - 4 * rq : y0;
-                if (two) d[x1] = y1 >= 4 * rq ? y1 - 4 * rq : y1;
+                const ulonglong2* matf = a.gmat_fp + a.gmat_off[g];
+#pragma unroll 2
+                for (uint32_t j = 0; j < LK - ag; ++j) {
+                    const uint32_t r = outl[j];
+                    const ulonglong2 fm = a.fmod[r];
+                    const double rd = as_f(fm.x), rinv = as_f(fm.y);
+                    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+                    for (uint32_t m = 0; m < AMAX; ++m)
+                        if (m < ag) {
+                            const ulonglong2 w = matf[j * ag + m];
+                            y0 = __dadd_rn(y0, fmulmod(td0[m], as_f(w.x), as_f(w.y), rd));
+                            y1 = __dadd_rn(y1, fmulmod(td1[m], as_f(w.x), as_f(w.y), rd));
+                        }
+                    uint64_t* d = dst0 + (size_t)r * a.N;
+                    d[x0] = f_to_u52(fcanon(freduce(y0, rd, rinv), rd));
+                    if (two) d[x1] = f_to_u52(fcanon(freduce(y1, rd, rinv), rd));
+                }
+            } else {
+#pragma unroll 2
+                for (uint32_t j = 0; j < LK - ag; ++j) {
+                    const uint32_t r = outl[j];
+                    const uint64_t rq = a.moduli[r], nq = 0 - rq;
+                    // sums of at most 8 lazy products in [0, 2 r): below 16 r < 2^64
+                    uint64_t y0 = 0, y1 = 0;
+#pragma unroll
+                    for (uint32_t m = 0; m < AMAX; ++m)
+                        if (m < ag) {
+                            const ulonglong2 w = mat[j * ag + m];
+                            y0 += shoup_lazy_nq(w.x, w.y, tv0[m], nq);
+                            y1 += shoup_lazy_nq(w.x, w.y, tv1[m], nq);
+                        }
+                    // [0, 4 r) is enough: the forward NTT that follows accepts inputs below
+                    // 4q and returns canonical values of the same residues
+                    if (AMAX > 4) {
+                        y0 = y0 >= 8 * rq ? y0 - 8 * rq : y0;
+                        y1 = y1 >= 8 * rq ? y1 - 8 * rq : y1;
+                    }
+                    uint64_t* d = dst0 + (size_t)r * a.N;
+                    d[x0] = y0 >= 4 * rq ? y0 - 4 * rq : y0;
+                    if (two) d[x1] = y1 >= 4 * rq ? y1 - 4 * rq : y1;
+                }
             }
         }
     }
@@ -144,6 +180,8 @@ struct PConvArgs {
     uint64_t* conv;        // [PC][L][N]
     const ulonglong2* pinv_k;
     const ulonglong2* pmat;     // [L][K]
+    const ulonglong2* pmat_fp;  // FP64 form of pmat (FP kernels)
+    const ulonglong2* fmod;     // [L+K] (q, 1/q) as doubles (FP kernels)
     const uint64_t* moduli;     // [L+K]
     const Barrett* bar;         // [L+K]
     size_t pc, N;
@@ -151,8 +189,9 @@ struct PConvArgs {
 };
 
 // fast conversion of the P limbs to the Q limbs, one thread per (poly, coefficient); grid y = poly.
-// KMAX bounds the special prime count (registers held per thread).
-template <uint32_t KMAX>
+// KMAX bounds the special prime count (registers held per thread).  FP: the dot
+// products on the FP64 pipe, as in modup_kernel.
+template <uint32_t KMAX, bool FP>
 __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
     for (size_t p = blockIdx.y; p < a.pc; p += gridDim.y) {
         const uint64_t* src = a.accp + (p * a.K) * a.N;
@@ -172,20 +211,44 @@ __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
                     if (two) tv1[k] = shoup_mul(f.x, f.y, src[(size_t)k * a.N + x1], pk);
                 }
             }
-#pragma unroll 2
-            for (uint32_t l = 0; l < a.L; ++l) {
-                const uint64_t ql = a.moduli[l], nq = 0 - ql;
-                // sums of at most 8 lazy products in [0, 2 q_l): below 16 q_l < 2^64
-                uint64_t y0 = 0, y1 = 0;
+            if constexpr (FP) {
+                double td0[KMAX], td1[KMAX];
 #pragma unroll
-                for (uint32_t k = 0; k < KMAX; ++k)
-                    if (k < a.K) {
-                        const ulonglong2 w = a.pmat[l * a.K + k];
-                        y0 += shoup_lazy_nq(w.x, w.y, tv0[k], nq);
-                        y1 += shoup_lazy_nq(w.x, w.y, tv1[k], nq);
-                    }
-                dst[(size_t)l * a.N + x0] = reduce_below_16q(y0, ql);
-                if (two) dst[(size_t)l * a.N + x1] = reduce_below_16q(y1, ql);
+                for (uint32_t k = 0; k < KMAX; ++k) {
+                    td0[k] = u52_to_f(tv0[k]);
+                    td1[k] = u52_to_f(tv1[k]);
+                }
+#pragma unroll 2
+                for (uint32_t l = 0; l < a.L; ++l) {
+                    const ulonglong2 fm = a.fmod[l];
+                    const double qd = as_f(fm.x), qinv = as_f(fm.y);
+                    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+                    for (uint32_t k = 0; k < KMAX; ++k)
+                        if (k < a.K) {
+                            const ulonglong2 w = a.pmat_fp[l * a.K + k];
+                            y0 = __dadd_rn(y0, fmulmod(td0[k], as_f(w.x), as_f(w.y), qd));
+                            y1 = __dadd_rn(y1, fmulmod(td1[k], as_f(w.x), as_f(w.y), qd));
+                        }
+                    dst[(size_t)l * a.N + x0] = f_to_u52(fcanon(freduce(y0, qd, qinv), qd));
+                    if (two) dst[(size_t)l * a.N + x1] = f_to_u52(fcanon(freduce(y1, qd, qinv), qd));
+                }
+            } else {
+#pragma unroll 2
+                for (uint32_t l = 0; l < a.L; ++l) {
+                    const uint64_t ql = a.moduli[l], nq = 0 - ql;
+                    // sums of at most 8 lazy products in [0, 2 q_l): below 16 q_l < 2^64
+                    uint64_t y0 = 0, y1 = 0;
+#pragma unroll
+                    for (uint32_t k = 0; k < KMAX; ++k)
+                        if (k < a.K) {
+                            const ulonglong2 w = a.pmat[l * a.K + k];
+                            y0 += shoup_lazy_nq(w.x, w.y, tv0[k], nq);
+                            y1 += shoup_lazy_nq(w.x, w.y, tv1[k], nq);
+                        }
+                    dst[(size_t)l * a.N + x0] = reduce_below_16q(y0, ql);
+                    if (two) dst[(size_t)l * a.N + x1] = reduce_below_16q(y1, ql);
+                }
             }
         }
     }
@@ -257,6 +320,17 @@ cudaError_t upload(T** d, const std::vector<T>& h) {
 }
 
 ulonglong2 shoup_pair(uint64_t w, uint64_t q) { return make_ulonglong2(w, h_shoup_quotient(w, q)); }
+
+// (a, b) as the bit patterns of two doubles
+ulonglong2 fp_bits(double a, double b) {
+    uint64_t x, y;
+    memcpy(&x, &a, 8);
+    memcpy(&y, &b, 8);
+    return make_ulonglong2(x, y);
+}
+
+// FP64 form of a Shoup pair (w, w') mod q: (w, w / q) as doubles
+ulonglong2 fp_pair(const ulonglong2& p, uint64_t q) { return fp_bits((double)p.x, (double)p.x / (double)q); }
 
 // product of moduli[idx] over idx in [lo, hi) except `skip`, mod r
 uint64_t prod_except(const std::vector<uint64_t>& m, uint32_t lo, uint32_t hi, uint32_t skip, uint64_t r) {
@@ -341,6 +415,25 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
         for (uint32_t k = 0; k < K; ++k) pmat[(size_t)l * K + k] = shoup_pair(prod_except(m, L, L + K, L + k, m[l]), m[l]);
         pinv[l] = shoup_pair(h_invmod(prod_except(m, L, L + K, UINT32_MAX, m[l]), m[l]), m[l]);
     }
+    // FP64 copies (every modulus below 2^50): matrices as (w, w / r), moduli as (q, 1/q)
+    uint64_t maxq = 0;
+    for (uint64_t q : m) maxq = std::max(maxq, q);
+    const bool fp = maxq < (1ull << 50);
+    std::vector<ulonglong2> gmat_fp, pmat_fp, fmod;
+    if (fp) {
+        for (uint32_t g = 0; g < h->dnum; ++g) {
+            const uint32_t lo = g * alpha, hi = std::min(L, lo + alpha), ag = hi - lo;
+            size_t idx = h->gmat_off[g], j = h->gout_off[g];
+            for (uint32_t r = 0; r < L + K; ++r) {
+                if (r >= lo && r < hi) continue;
+                for (uint32_t i = 0; i < ag; ++i, ++idx) gmat_fp.push_back(fp_pair(gmat[idx], m[gout[j]]));
+                ++j;
+            }
+        }
+        for (uint32_t l = 0; l < L; ++l)
+            for (uint32_t k = 0; k < K; ++k) pmat_fp.push_back(fp_pair(pmat[(size_t)l * K + k], m[l]));
+        for (uint32_t i = 0; i < L + K; ++i) fmod.push_back(fp_bits((double)m[i], 1.0 / (double)m[i]));
+    }
     std::vector<uint32_t> offs(h->gmat_off);
     offs.insert(offs.end(), h->gout_off.begin(), h->gout_off.end());
     cudaError_t e = upload(&h->d_ginv, ginv);
@@ -350,6 +443,9 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
     if (e == cudaSuccess) e = upload(&h->d_pmat, pmat);
     if (e == cudaSuccess) e = upload(&h->d_pinv, pinv);
     if (e == cudaSuccess) e = upload(&h->d_offs, offs);
+    if (e == cudaSuccess && fp) e = upload(&h->d_gmat_fp, gmat_fp);
+    if (e == cudaSuccess && fp) e = upload(&h->d_pmat_fp, pmat_fp);
+    if (e == cudaSuccess && fp) e = upload(&h->d_fmod, fmod);
     if (e != cudaSuccess) {
         pg_hybrid_ks_destroy(h);
         return cuda_status(e, "pg_hybrid_ks_create: upload");
@@ -367,6 +463,9 @@ int pg_hybrid_ks_destroy(pg_hybrid_ks* h) {
     cudaFree(h->d_pmat);
     cudaFree(h->d_pinv);
     cudaFree(h->d_offs);
+    cudaFree(h->d_gmat_fp);
+    cudaFree(h->d_pmat_fp);
+    cudaFree(h->d_fmod);
     delete h;
     return PG_OK;
 }
@@ -424,10 +523,16 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     ma.alpha = h->alpha;
     ma.dnum = h->dnum;
     ma.log_n = t->log_n;
+    // the FP64 dot products when the table runs the FP64 schedule (every modulus below 2^50)
+    const bool fp = h->d_fmod && t->fp64;
+    ma.gmat_fp = h->d_gmat_fp;
+    ma.fmod = h->d_fmod;
+    const dim3 mgrid = grid2((n + 1) / 2, ma.polys * h->dnum);
     if (h->alpha <= 4)
-        modup_kernel<4><<<grid2((n + 1) / 2, ma.polys * h->dnum), 256, 0, st>>>(ma);
+        fp ? modup_kernel<4, true><<<mgrid, 256, 0, st>>>(ma) : modup_kernel<4, false><<<mgrid, 256, 0, st>>>(ma);
     else
-        modup_kernel<kMaxAlpha><<<grid2((n + 1) / 2, ma.polys * h->dnum), 256, 0, st>>>(ma);
+        fp ? modup_kernel<kMaxAlpha, true><<<mgrid, 256, 0, st>>>(ma)
+           : modup_kernel<kMaxAlpha, false><<<mgrid, 256, 0, st>>>(ma);
     count_launch();
     PG_LAUNCH_CHECK("modup_kernel launch");
     int rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
@@ -451,10 +556,13 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     pa.L = h->L;
     pa.K = h->K;
     pa.log_n = t->log_n;
+    pa.pmat_fp = h->d_pmat_fp;
+    pa.fmod = h->d_fmod;
+    const dim3 pgrid = grid2((n + 1) / 2, pa.pc);
     if (h->K <= 4)
-        pconv_kernel<4><<<grid2((n + 1) / 2, pa.pc), 256, 0, st>>>(pa);
+        fp ? pconv_kernel<4, true><<<pgrid, 256, 0, st>>>(pa) : pconv_kernel<4, false><<<pgrid, 256, 0, st>>>(pa);
     else
-        pconv_kernel<kMaxK><<<grid2((n + 1) / 2, pa.pc), 256, 0, st>>>(pa);
+        fp ? pconv_kernel<kMaxK, true><<<pgrid, 256, 0, st>>>(pa) : pconv_kernel<kMaxK, false><<<pgrid, 256, 0, st>>>(pa);
     count_launch();
     PG_LAUNCH_CHECK("pconv_kernel launch");
     rc = launch_ntt(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, MODE_FWD, st);

@@ -42,6 +42,32 @@ def test_hybrid_key_switch_bit_exact(gpu, log_n, L, K, alpha, k_in, k_out, batch
     do2 = gpu.DeviceBuffer(batch * per_out)
     hks.key_switch(k_in, k_out, dk, di, do2, batch, workspace=ws)
     assert np.array_equal(do2.numpy(), exp)
+    # the integer-only schedule (FP64 off: NTTs and base conversions on the integer pipe)
+    table.set_fp64(False)
+    do3 = gpu.DeviceBuffer(batch * per_out)
+    hks.key_switch(k_in, k_out, dk, di, do3, batch)
+    assert np.array_equal(do3.numpy(), exp)
+
+
+def test_hybrid_key_switch_wide_moduli(gpu):
+    """Moduli between 2^50 and 2^59 run every step on the integer pipe."""
+    log_n, L, K, alpha, k_in, k_out, batch = 10, 5, 2, 2, 1, 1, 2
+    n = 1 << log_n
+    moduli = O.ntt_primes(1 << 58, 2 * n, L + K)
+    ref = O.HybridKeySwitch(log_n, moduli, L, K, alpha)
+    table = gpu.DcrtTable(log_n, moduli)
+    assert not table.fp64
+    hks = gpu.HybridKeySwitch(table, L, K, alpha)
+    rows = k_in * hks.dnum * (k_out + 1)
+    key = np.concatenate([O.uniform_rns(0x4C, 50 * r, moduli, n).ravel() for r in range(rows)])
+    c_in = np.concatenate([O.uniform_rns(0x1D, 40 * b + 20 * i, moduli[:L], n).ravel()
+                           for b in range(batch) for i in range(k_in + 1)])
+    per_in, per_out = (k_in + 1) * L * n, (k_out + 1) * L * n
+    exp = np.concatenate([ref.key_switch(k_in, k_out, key, c_in[b * per_in:(b + 1) * per_in])
+                          for b in range(batch)])
+    do = gpu.DeviceBuffer(batch * per_out)
+    hks.key_switch(k_in, k_out, gpu.DeviceBuffer.from_numpy(key), gpu.DeviceBuffer.from_numpy(c_in), do, batch)
+    assert np.array_equal(do.numpy(), exp)
 
 
 def test_hybrid_key_switch_decrypts(gpu):
