@@ -71,8 +71,11 @@ struct MacArgs {
 constexpr uint32_t kMacChunk = 2;
 constexpr uint32_t kMacOut = 2;
 
-template <bool FOLD>
-__global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
+// NEG: the key-switch form (base - sum, base = add_last on the last output); SPLIT:
+// limbs >= l_split written to out_hi (hybrid key switch).  Compile-time, so that
+// each launch carries only its own epilogue.
+template <bool FOLD, bool NEG, bool SPLIT>
+__global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
     const uint32_t LN = a.L * (uint32_t)a.N;
     const uint32_t pairs = (a.KOUT + kMacOut - 1) / kMacOut;
     const size_t outer = ((a.B + kMacChunk - 1) / kMacChunk) * pairs;
@@ -125,19 +128,19 @@ __global__ void __launch_bounds__(256) mac_kernel(MacArgs a) {
                     const size_t bc = b * a.KOUT + c;
                     const uint64_t s = barrett_reduce_128(lo[cc][bb], hi[cc][bb], m);
                     uint64_t r;
-                    if (a.negate) {
+                    if constexpr (NEG) {
                         const uint64_t base = (a.add_last && c == a.KOUT - 1) ? a.add_last[b * LN + lx] : 0;
                         r = sub_mod(base, s, m.q);
                     } else {
                         const uint64_t base = a.acc ? a.acc[bc * LN + lx] : 0;
                         r = add_mod(base, s, m.q);
                     }
-                    if (a.out_hi) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
-                        const uint32_t x = lx & ((uint32_t)a.N - 1);
-                        if (l < a.l_split)
-                            a.out[(bc * a.l_split + l) * a.N + x] = r;
-                        else
-                            a.out_hi[(bc * (a.L - a.l_split) + (l - a.l_split)) * a.N + x] = r;
+                    if constexpr (SPLIT) {  // split output: [B][KOUT][l_split][N] and [B][KOUT][L - l_split][N]
+                        const bool lo_part = l < a.l_split;
+                        uint64_t* dst = lo_part ? a.out : a.out_hi;
+                        const size_t limbs = lo_part ? a.l_split : a.L - a.l_split;
+                        const uint32_t lrow = lo_part ? l : l - a.l_split;
+                        dst[(bc * limbs + lrow) * a.N + (lx & ((uint32_t)a.N - 1))] = r;
                     } else {
                         a.out[bc * LN + lx] = r;
                     }
@@ -265,10 +268,18 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     if ((size_t)t->L * t->n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
     const size_t LN = (size_t)t->L * t->n;
     const dim3 grid = grid2(LN, ((B + kMacChunk - 1) / kMacChunk) * ((kout + kMacOut - 1) / kMacOut));
-    if (kin * d > 8)  // more than 8 products per output: fold the 128-bit sums every 8
-        mac_kernel<true><<<grid, 256, 0, st>>>(a);
-    else
-        mac_kernel<false><<<grid, 256, 0, st>>>(a);
+    const bool fold = kin * d > 8;  // more than 8 products per output: fold the 128-bit sums every 8
+    if (out_hi) {
+        if (negate) return set_error(PG_ERR_INVALID_ARGUMENT, "split MAC output has no key-switch form");
+        fold ? mac_kernel<true, false, true><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, false, true><<<grid, 256, 0, st>>>(a);
+    } else if (negate) {
+        fold ? mac_kernel<true, true, false><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, true, false><<<grid, 256, 0, st>>>(a);
+    } else {
+        fold ? mac_kernel<true, false, false><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, false, false><<<grid, 256, 0, st>>>(a);
+    }
     count_launch();
     PG_LAUNCH_CHECK("mac_kernel launch");
     return PG_OK;
