@@ -86,7 +86,7 @@ struct ModUpArgs {
 // run on the FP64 pipe (fmulmod, every modulus below 2^50): each product lies in
 // (-0.75 r, 0.75 r), a sum of at most 8 below 6 r < 2^53, reduced exactly to [0, r).
 template <uint32_t AMAX, bool FP>
-__global__ void __launch_bounds__(256) modup_kernel(ModUpArgs a) {
+__global__ void __launch_bounds__(256, 3) modup_kernel(ModUpArgs a) {
     const uint32_t LK = a.L + a.K;
     const size_t outer = a.polys * a.dnum;
     for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
