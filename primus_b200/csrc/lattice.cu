@@ -82,14 +82,19 @@ __global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
     const size_t kstride = (size_t)a.KOUT * LN;
     const size_t dstride = (size_t)a.KIN * a.d * LN;  // one ciphertext's digits
     const uint32_t nterms = a.KIN * a.d;
-    for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
-        const uint32_t c0 = (uint32_t)(o % pairs) * kMacOut;
-        const uint32_t nc = min(kMacOut, a.KOUT - c0);
-        const size_t b0 = (o / pairs) * kMacChunk;
-        const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
-        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
-            const uint32_t l = lx >> a.log_n;
-            const Barrett m = a.bar[l];
+    // grid x runs over (chunk, output pair) and y over coefficient tiles: CTAs
+    // launched next to each other share one tile of the key, which then comes
+    // from L2 for every chunk after the first
+    for (uint32_t lx0 = blockIdx.y * blockDim.x; lx0 < LN; lx0 += gridDim.y * blockDim.x) {
+        const uint32_t lx = lx0 + threadIdx.x;
+        if (lx >= LN) break;
+        const uint32_t l = lx >> a.log_n;
+        const Barrett m = a.bar[l];
+        for (size_t o = blockIdx.x; o < outer; o += gridDim.x) {
+            const uint32_t c0 = (uint32_t)(o % pairs) * kMacOut;
+            const uint32_t nc = min(kMacOut, a.KOUT - c0);
+            const size_t b0 = (o / pairs) * kMacChunk;
+            const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
             uint64_t lo[kMacOut][kMacChunk], hi[kMacOut][kMacChunk];
 #pragma unroll
             for (uint32_t cc = 0; cc < kMacOut; ++cc)
@@ -267,7 +272,9 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     a.negate = negate;
     if ((size_t)t->L * t->n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
     const size_t LN = (size_t)t->L * t->n;
-    const dim3 grid = grid2(LN, ((B + kMacChunk - 1) / kMacChunk) * ((kout + kMacOut - 1) / kMacOut));
+    const size_t outer = ((B + kMacChunk - 1) / kMacChunk) * ((kout + kMacOut - 1) / kMacOut);
+    const dim3 grid((unsigned)std::min<size_t>(outer, 0x7fffffff),
+                    (unsigned)std::min<size_t>((LN + 255) / 256, 65535));
     const bool fold = kin * d > 8;  // more than 8 products per output: fold the 128-bit sums every 8
     if (out_hi) {
         if (negate) return set_error(PG_ERR_INVALID_ARGUMENT, "split MAC output has no key-switch form");
