@@ -280,6 +280,13 @@ int pg_rns_decompose(const pg_rns_base *base, const uint64_t *d_values, uint64_t
 int pg_rns_wrapping_decompose_small(const pg_rns_base *base, const uint64_t *d_small,
                                     uint64_t *d_residues, size_t count, uint64_t small_modulus,
                                     void *stream);
+/* dest[l][x] = dest[l][x] + factor[l] * lift_l(small[x]) mod q_l, the lift as above
+ * (add_wrapping_decompose_small_values_scaled, base.rs:238-283: the same values as
+ * the lift followed by add_mul_factor, without the lifted copy).  h_factor: [L]
+ * host scalars below their moduli; dest: [L][count] canonical. */
+int pg_rns_add_wrapping_decompose_small_scaled(const pg_rns_base *base, const uint64_t *d_small,
+                                               uint64_t *d_dest, size_t count, uint64_t small_modulus,
+                                               const uint64_t *h_factor, void *stream);
 
 /* ------------------------------------------------------ fast base conversion
  * BaseConverter (primus_rns/src/converter.rs:12-47); fast_convert_array

@@ -258,6 +258,25 @@ __global__ void __launch_bounds__(256) wrap_small_kernel(const uint64_t* __restr
     }
 }
 
+// add_wrapping_decompose_small_values_scaled (base.rs:238-283): dest[l][x] +=
+// factor_l * lift_l(small[x]) mod q_l, the lift as in wrap_small_kernel and the
+// product by the Shoup-prepared factor (f, f') canonical, so the sum is too.
+// Grid-stride over [L][count], one 16-byte factor load per element.
+__global__ void __launch_bounds__(256) add_wrap_scaled_kernel(const uint64_t* __restrict__ small,
+                                                              uint64_t* __restrict__ dest, size_t count, uint32_t L,
+                                                              const uint64_t* __restrict__ moduli,
+                                                              const ulonglong2* __restrict__ factor, uint64_t sm) {
+    const size_t total = count * L;
+    const uint64_t half = (sm + 1) / 2;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)(t / count);
+        const uint64_t q = moduli[i], v = small[t % count];
+        const uint64_t lifted = (sm == 2 || v < half) ? v : q - sm + v;
+        const ulonglong2 f = factor[i];
+        dest[t] = add_mod(dest[t], shoup_mul(f.x, f.y, lifted, q), q);
+    }
+}
+
 // fast_convert_array (converter.rs:147-175): y_j = sum_i buf_i * M[j][i] mod p_j,
 // buf_i = [x_i * (Q/q_i)^-1]_{q_i}; 128-bit accumulation folded every 8 terms
 __global__ void __launch_bounds__(256) fast_convert_kernel(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
@@ -566,6 +585,37 @@ int pg_rns_wrapping_decompose_small(const pg_rns_base* b, const uint64_t* d_smal
                                                                                      b->d_moduli, small_modulus);
     count_launch();
     PG_LAUNCH_CHECK("wrap_small_kernel launch");
+    return PG_OK;
+}
+
+int pg_rns_add_wrapping_decompose_small_scaled(const pg_rns_base* b, const uint64_t* d_small, uint64_t* d_dest,
+                                               size_t count, uint64_t small_modulus, const uint64_t* h_factor,
+                                               void* stream) {
+    if (!b) return set_error(PG_ERR_INVALID_ARGUMENT, "base is NULL");
+    if (count == 0) return PG_OK;
+    if (!d_small || !d_dest || !h_factor) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (small_modulus < 2) return set_error(PG_ERR_INVALID_ARGUMENT, "small_modulus must be at least 2");
+    std::vector<ulonglong2> f(b->L);
+    for (uint32_t l = 0; l < b->L; ++l) {
+        const uint64_t q = b->moduli[l];
+        if (q <= small_modulus) return set_error(PG_ERR_INVALID_ARGUMENT, "every modulus must exceed small_modulus");
+        if (h_factor[l] >= q) return set_error(PG_ERR_INVALID_ARGUMENT, "factor not below its modulus");
+        f[l] = make_ulonglong2(h_factor[l], h_shoup_quotient(h_factor[l], q));
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    void* d_f = nullptr;
+    PG_CUDA(scratch_alloc(&d_f, b->L * sizeof(ulonglong2), st));
+    // pageable source: the copy below completes before the call returns
+    cudaError_t e = cudaMemcpyAsync(d_f, f.data(), b->L * sizeof(ulonglong2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        add_wrap_scaled_kernel<<<grid_for(count * b->L, 256), 256, 0, st>>>(d_small, d_dest, count, b->L,
+                                                                             b->d_moduli, (const ulonglong2*)d_f,
+                                                                             small_modulus);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    scratch_free(d_f, st);
+    if (e != cudaSuccess) return cuda_status(e, "add_wrap_scaled_kernel");
     return PG_OK;
 }
 

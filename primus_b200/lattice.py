@@ -69,6 +69,13 @@ class RnsBase:
                                  stream=None):
         call("pg_rns_wrapping_decompose_small", self.h, small.ptr, residues.ptr, count, small_modulus, _sh(stream))
 
+    def add_wrapping_decompose_small_scaled(self, small: DeviceBuffer, dest: DeviceBuffer, count: int,
+                                            small_modulus: int, factor, stream=None):
+        """RNSBase::add_wrapping_decompose_small_values_scaled: dest += factor * lift(small)."""
+        f = np.ascontiguousarray(np.asarray(factor, dtype=np.uint64))
+        call("pg_rns_add_wrapping_decompose_small_scaled", self.h, small.ptr, dest.ptr, count, small_modulus, ptr(f),
+             _sh(stream))
+
 
 class BaseConverter:
     def __init__(self, ibase: RnsBase, obase: RnsBase):

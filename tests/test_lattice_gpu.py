@@ -59,6 +59,29 @@ def test_wrapping_decompose_small(gpu):
         assert np.array_equal(out.numpy((2, small.size)), ref.wrapping_decompose_small(small, t))
 
 
+def test_add_wrapping_decompose_small_scaled(gpu):
+    """RNSBase::add_wrapping_decompose_small_values_scaled (base.rs:238-283) equals the
+    lift followed by the per-limb scaled add (the oracle's two steps), for t = 2 (no
+    centering) and odd / even t, with factors at 0, 1 and q - 1 among them."""
+    moduli = O.ntt_primes(1 << 50, 1 << 12, 3)
+    base = gpu.RnsBase(moduli)
+    ref = O.RnsBase(moduli)
+    n = 3000
+    for t, factor in ((2, [5, 0, moduli[2] - 1]), (257, [1, moduli[1] - 1, 12345]), (4096, [7, 8, 9])):
+        small = O.uniform(11, t, t, n)
+        dest = O.uniform_rns(12, t, moduli, n)
+        lifted = ref.wrapping_decompose_small(small, t)
+        exp = dest.copy()
+        for l, q in enumerate(moduli):
+            exp[l] = O.add_mul_scalar(dest[l], lifted[l], factor[l], q)
+        dd = gpu.DeviceBuffer.from_numpy(dest)
+        base.add_wrapping_decompose_small_scaled(gpu.DeviceBuffer.from_numpy(small), dd, n, t, factor)
+        assert np.array_equal(dd.numpy(dest.shape), exp), t
+    with pytest.raises(gpu.PrimusGpuError):
+        base.add_wrapping_decompose_small_scaled(gpu.DeviceBuffer.from_numpy(small), dd, n, 4096,
+                                                 [moduli[0], 1, 1])  # factor not below its modulus
+
+
 @pytest.mark.parametrize("li,lo", [(2, 2), (4, 3), (16, 4), (24, 2)])
 def test_fast_convert(gpu, li, lo):
     qs = O.ntt_primes(1 << 50, 1 << 13, li)
