@@ -557,7 +557,7 @@ def bench_hybrid_ks(P, stream, batches=(1, 8, 32)):
     key = P.DeviceBuffer(hks.dnum * 2 * 20 * 32768)
     kt.fill_uniform(key, hks.dnum * 2, seed=0x5EED0006, stream=stream)
     res = {"workload": "hybrid key switch, N=2^15, L=16 + K=4 special primes, alpha=4 (dnum=4), k=1",
-           "rows_transformed_per_key_switch": 4 * 20 + 4 * 2 + 16 * 2 + 16}
+           "rows_transformed_per_key_switch": 4 * 20 + 4 * 2 + 16 * 2}
     for B in batches:
         di, do = P.DeviceBuffer(B * 2 * 16 * 32768), P.DeviceBuffer(B * 2 * 16 * 32768)
         kq.fill_uniform(di, 2 * B, seed=0x5EED0007, stream=stream)

@@ -16,13 +16,19 @@
 //     forward NTT, then (acc_Q - conv) * P^-1 mod q_l
 //   c_out = -ModDown(acc) + (0, .., NTT(b))           (the reference's sign form)
 //
+// Evaluated through the linearity of the NTT as
+//   c_out[c] = NTT(P^-1 conv[c] + [c = last] b) - P^-1 acc_Q[c]
+// (P^-1 folded into the conversion matrix, b added in coefficient form), so b
+// needs no transform of its own; the residues are the same.
+//
 // The key row [i][g] encrypts P * (Q/Q_g) * ((Q/Q_g)^-1 mod Q_g) * s_in_i under
 // s_out over QP, i.e. [P]_{q_l} * s_in_i on the limbs of D_g and 0 elsewhere.
 //
 // Launch sequence for a batch: modup_kernel -> forward NTT of every extended
 // row -> the MAC kernel (Q and P limbs written apart) -> inverse NTT of the P
-// limbs -> pconv_kernel (P -> Q) -> forward NTT of the converted rows and of b
-// -> finish_kernel.  Each step runs over the whole batch in one launch.
+// limbs -> pconv_kernel (P -> Q, scaled by P^-1, b added on the last output)
+// -> forward NTT of the converted rows -> finish_kernel.  Each step runs over
+// the whole batch in one launch.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -46,7 +52,7 @@ struct pg_hybrid_ks {
     uint32_t* d_gout = nullptr;    // per group g: [L+K-alpha_g] output limb indices, at gout_off[g]
     std::vector<uint32_t> gmat_off, gout_off;
     ulonglong2* d_pinv_k = nullptr;  // [K] Shoup pair of ((P/p_k)^-1 mod p_k)
-    ulonglong2* d_pmat = nullptr;    // [L][K] Shoup pair of (P/p_k) mod q_l
+    ulonglong2* d_pmat = nullptr;    // [L][K] Shoup pair of (P/p_k) * P^-1 mod q_l
     ulonglong2* d_pinv = nullptr;    // [L] Shoup pair of (P^-1 mod q_l)
     uint32_t* d_offs = nullptr;      // [2 * dnum]: gmat_off then gout_off
     // FP64 copies for moduli below 2^50: (w, w / r) as doubles, and (q, 1/q) per limb
@@ -178,6 +184,9 @@ __global__ void __launch_bounds__(256, 3) modup_kernel(ModUpArgs a) {
 struct PConvArgs {
     const uint64_t* accp;  // [PC][K][N], coefficient form
     uint64_t* conv;        // [PC][L][N]
+    const uint64_t* bsrc;  // b of ciphertext j at bsrc + j * bstride ([L][N], coefficient form)
+    size_t bstride;
+    uint32_t ko;           // output polys per ciphertext (b goes to the last)
     const ulonglong2* pinv_k;
     const ulonglong2* pmat;     // [L][K]
     const ulonglong2* pmat_fp;  // FP64 form of pmat (FP kernels)
@@ -196,6 +205,8 @@ __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
     for (size_t p = blockIdx.y; p < a.pc; p += gridDim.y) {
         const uint64_t* src = a.accp + (p * a.K) * a.N;
         uint64_t* dst = a.conv + (p * a.L) * a.N;
+        // the last output poly of each ciphertext also takes b (coefficient form)
+        const uint64_t* bp = (p % a.ko) == a.ko - 1 ? a.bsrc + (p / a.ko) * a.bstride : nullptr;
         // two coefficients per thread (x and x + blockDim.x)
         for (uint32_t x0 = blockIdx.x * 2 * blockDim.x + threadIdx.x; x0 < a.N; x0 += gridDim.x * 2 * blockDim.x) {
             const uint32_t x1 = x0 + blockDim.x;
@@ -230,8 +241,15 @@ __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
                             y0 = __dadd_rn(y0, fmulmod(td0[k], as_f(w.x), as_f(w.y), qd));
                             y1 = __dadd_rn(y1, fmulmod(td1[k], as_f(w.x), as_f(w.y), qd));
                         }
-                    dst[(size_t)l * a.N + x0] = f_to_u52(fcanon(freduce(y0, qd, qinv), qd));
-                    if (two) dst[(size_t)l * a.N + x1] = f_to_u52(fcanon(freduce(y1, qd, qinv), qd));
+                    uint64_t r0 = f_to_u52(fcanon(freduce(y0, qd, qinv), qd));
+                    uint64_t r1 = two ? f_to_u52(fcanon(freduce(y1, qd, qinv), qd)) : 0;
+                    if (bp) {
+                        const uint64_t ql = a.moduli[l];
+                        r0 = add_mod(r0, bp[(size_t)l * a.N + x0], ql);
+                        if (two) r1 = add_mod(r1, bp[(size_t)l * a.N + x1], ql);
+                    }
+                    dst[(size_t)l * a.N + x0] = r0;
+                    if (two) dst[(size_t)l * a.N + x1] = r1;
                 }
             } else {
 #pragma unroll 2
@@ -246,8 +264,14 @@ __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
                             y0 += shoup_lazy_nq(w.x, w.y, tv0[k], nq);
                             y1 += shoup_lazy_nq(w.x, w.y, tv1[k], nq);
                         }
-                    dst[(size_t)l * a.N + x0] = reduce_below_16q(y0, ql);
-                    if (two) dst[(size_t)l * a.N + x1] = reduce_below_16q(y1, ql);
+                    uint64_t r0 = reduce_below_16q(y0, ql);
+                    uint64_t r1 = two ? reduce_below_16q(y1, ql) : 0;
+                    if (bp) {
+                        r0 = add_mod(r0, bp[(size_t)l * a.N + x0], ql);
+                        if (two) r1 = add_mod(r1, bp[(size_t)l * a.N + x1], ql);
+                    }
+                    dst[(size_t)l * a.N + x0] = r0;
+                    if (two) dst[(size_t)l * a.N + x1] = r1;
                 }
             }
         }
@@ -256,8 +280,7 @@ __global__ void __launch_bounds__(256) pconv_kernel(PConvArgs a) {
 
 struct FinishArgs {
     const uint64_t* accq;  // [B][KO][L][N]
-    const uint64_t* conv;  // [B][KO][L][N] NTT domain
-    const uint64_t* bt;    // [B][L][N] NTT(b)
+    const uint64_t* conv;  // [B][KO][L][N] NTT(P^-1 conv + [last] b)
     uint64_t* out;         // [B][KO][L][N]
     const ulonglong2* pinv;
     const uint64_t* moduli;
@@ -265,23 +288,19 @@ struct FinishArgs {
     uint32_t KO, L, log_n;
 };
 
-// out = (c == KO-1 ? NTT(b) : 0) - (acc_Q - conv) * P^-1; grid y = b * KO + c
+// out = NTT(P^-1 conv + [c = last] b) - acc_Q * P^-1; grid y = b * KO + c
 __global__ void __launch_bounds__(256) finish_kernel(FinishArgs a) {
     const uint32_t LN = a.L * (uint32_t)a.N;
     const size_t outer = a.B * a.KO;
     for (size_t o = blockIdx.y; o < outer; o += gridDim.y) {
-        const bool last = (o % a.KO) == a.KO - 1;
-        const size_t b = o / a.KO;
         const uint64_t* aq = a.accq + o * LN;
         const uint64_t* cv = a.conv + o * LN;
-        const uint64_t* bt = a.bt + b * LN;
         uint64_t* out = a.out + o * LN;
         for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
             const uint32_t l = lx >> a.log_n;
             const uint64_t q = a.moduli[l];
             const ulonglong2 f = a.pinv[l];
-            const uint64_t v = shoup_mul(f.x, f.y, sub_mod(aq[lx], cv[lx], q), q);
-            out[lx] = sub_mod(last ? bt[lx] : 0, v, q);
+            out[lx] = sub_mod(cv[lx], shoup_mul(f.x, f.y, aq[lx], q), q);
         }
     }
 }
@@ -340,10 +359,10 @@ uint64_t prod_except(const std::vector<uint64_t>& m, uint32_t lo, uint32_t hi, u
     return p;
 }
 
-// scratch words: ext | accQ | accP | conv | bt
+// scratch words: ext | accQ | accP | conv
 struct HybridWs {
-    size_t ext, accq, accp, conv, bt;
-    size_t total() const { return ext + accq + accp + conv + bt; }
+    size_t ext, accq, accp, conv;
+    size_t total() const { return ext + accq + accp + conv; }
 };
 
 HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t batch) {
@@ -353,7 +372,6 @@ HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t 
     w.accq = batch * KO * h->L * n;
     w.accp = batch * KO * h->K * n;
     w.conv = batch * KO * h->L * n;
-    w.bt = batch * h->L * n;
     return w;
 }
 
@@ -412,8 +430,10 @@ int pg_hybrid_ks_create(const pg_ntt_table* t, uint32_t L, uint32_t K, uint32_t 
     for (uint32_t k = 0; k < K; ++k)
         pinv_k[k] = shoup_pair(h_invmod(prod_except(m, L, L + K, L + k, m[L + k]), m[L + k]), m[L + k]);
     for (uint32_t l = 0; l < L; ++l) {
-        for (uint32_t k = 0; k < K; ++k) pmat[(size_t)l * K + k] = shoup_pair(prod_except(m, L, L + K, L + k, m[l]), m[l]);
-        pinv[l] = shoup_pair(h_invmod(prod_except(m, L, L + K, UINT32_MAX, m[l]), m[l]), m[l]);
+        const uint64_t pi = h_invmod(prod_except(m, L, L + K, UINT32_MAX, m[l]), m[l]);  // P^-1 mod q_l
+        pinv[l] = shoup_pair(pi, m[l]);
+        for (uint32_t k = 0; k < K; ++k)
+            pmat[(size_t)l * K + k] = shoup_pair(h_mulmod(prod_except(m, L, L + K, L + k, m[l]), pi, m[l]), m[l]);
     }
     // FP64 copies (every modulus below 2^50): matrices as (w, w / r), moduli as (q, 1/q)
     uint64_t maxq = 0;
@@ -503,7 +523,6 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     uint64_t* accq = ext + w.ext;
     uint64_t* accp = accq + w.accq;
     uint64_t* conv = accp + w.accp;
-    uint64_t* bt = conv + w.conv;
     // ModUp of every mask of every ciphertext, all groups
     ModUpArgs ma{};
     ma.in = d_in;
@@ -558,6 +577,9 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     pa.log_n = t->log_n;
     pa.pmat_fp = h->d_pmat_fp;
     pa.fmod = h->d_fmod;
+    pa.bsrc = d_in + (size_t)k_in * L * n;  // b of ciphertext j: after its k_in masks
+    pa.bstride = (size_t)(k_in + 1) * L * n;
+    pa.ko = (uint32_t)KO;
     const dim3 pgrid = grid2((n + 1) / 2, pa.pc);
     if (h->K <= 4)
         fp ? pconv_kernel<4, true><<<pgrid, 256, 0, st>>>(pa) : pconv_kernel<4, false><<<pgrid, 256, 0, st>>>(pa);
@@ -565,17 +587,12 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
         fp ? pconv_kernel<kMaxK, true><<<pgrid, 256, 0, st>>>(pa) : pconv_kernel<kMaxK, false><<<pgrid, 256, 0, st>>>(pa);
     count_launch();
     PG_LAUNCH_CHECK("pconv_kernel launch");
+    // NTT(P^-1 conv + [last] b): b reaches the NTT domain through the same transform
     rc = launch_ntt(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, MODE_FWD, st);
-    if (rc) return rc;
-    // b of every input, moved to the NTT domain
-    PG_CUDA(cudaMemcpy2DAsync(bt, L * n * 8, d_in + (size_t)k_in * L * n, (size_t)(k_in + 1) * L * n * 8, L * n * 8,
-                              batch, cudaMemcpyDeviceToDevice, st));
-    rc = launch_ntt(make_args(&h->tq, bt, batch * L, 0), t->log_n, MODE_FWD, st);
     if (rc) return rc;
     FinishArgs fa{};
     fa.accq = accq;
     fa.conv = conv;
-    fa.bt = bt;
     fa.out = d_out;
     fa.pinv = h->d_pinv;
     fa.moduli = t->d_moduli;
