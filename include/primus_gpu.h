@@ -530,8 +530,9 @@ int pg_polymul_batch_run(pg_polymul_batch *batch, const pg_polymul_job *h_jobs, 
  * stream plus an equal share of memory_budget_bytes of scratch) is free, taking
  * as many pending requests as fit the slot's scratch (admission by memory), so
  * requests that arrive while others run join the next batch and batches on
- * different slots overlap.  Completion is signalled by a host callback on the
- * slot's stream.  Results are identical to running each request alone. */
+ * different slots overlap.  A completion thread polls each batch's event and
+ * then marks its requests done.  Results are identical to running each request
+ * alone. */
 enum { PG_REQ_POLYMUL = 1, PG_REQ_EXT_PRODUCT = 2, PG_REQ_KEY_SWITCH = 3 };
 
 typedef struct pg_request {
