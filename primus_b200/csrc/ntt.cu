@@ -207,7 +207,8 @@ template <typename DT, bool FAST>
 static int launch_ext_fused_n(const ExtFusedArgs& a, uint32_t log_n, size_t smem, cudaStream_t st) {
     switch (log_n) {
         case 10: return launch_ext_fused_t<10, 3, DT, FAST>(a, smem, st);
-        case 11: return launch_ext_fused_t<11, 3, DT, FAST>(a, smem, st);
+        // 2^11: E = 4 (512 threads, 64 registers, two CTAs per SM) beats E = 8 by 4.5%
+        case 11: return launch_ext_fused_t<11, 2, DT, FAST>(a, smem, st);
         case 12: return launch_ext_fused_t<12, 3, DT, FAST>(a, smem, st);
         default: return set_error(PG_ERR_UNSUPPORTED, "fused external product: log_n outside 10..12");
     }
