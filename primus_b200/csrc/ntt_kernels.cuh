@@ -194,6 +194,24 @@ PG_DEV void inv_bfly_fp(uint64_t& x, uint64_t& y, const ulonglong2 w, double q, 
     y = as_u(fmulmod(__dsub_rn(u, v), as_f(w.x), as_f(w.y), q));
 }
 
+// Two Gentleman-Sande stages at once on (x0, x1, x2, x3) (stage p pairs (x0, x1)
+// with wa and (x2, x3) with wb, stage p+1 pairs the results (0, 2) and (1, 3)
+// with wc), inputs below q in magnitude: the stage-p sums (< 2q) are not
+// reduced; the stage-(p+1) sums and the difference s01 - s23 (< 4q) are, so
+// every product's input stays below 2^51 and the outputs below 0.75 q.
+// 41 FP64 operations for four butterflies instead of 44.
+PG_DEV void inv_bfly4_fp(uint64_t& x0, uint64_t& x1, uint64_t& x2, uint64_t& x3, const ulonglong2 wa,
+                         const ulonglong2 wb, const ulonglong2 wc, double q, double qinv) {
+    const double a0 = as_f(x0), a1 = as_f(x1), a2 = as_f(x2), a3 = as_f(x3);
+    const double s01 = __dadd_rn(a0, a1), s23 = __dadd_rn(a2, a3);
+    const double d01 = fmulmod(__dsub_rn(a0, a1), as_f(wa.x), as_f(wa.y), q);
+    const double d23 = fmulmod(__dsub_rn(a2, a3), as_f(wb.x), as_f(wb.y), q);
+    x0 = as_u(freduce(__dadd_rn(s01, s23), q, qinv));
+    x2 = as_u(fmulmod(freduce(__dsub_rn(s01, s23), q, qinv), as_f(wc.x), as_f(wc.y), q));
+    x1 = as_u(freduce(__dadd_rn(d01, d23), q, qinv));
+    x3 = as_u(fmulmod(__dsub_rn(d01, d23), as_f(wc.x), as_f(wc.y), q));
+}
+
 // last inverse stage fused with N^-1; writes canonical integers (not doubles)
 PG_DEV void inv_last_bfly_fp(uint64_t& x, uint64_t& y, const ulonglong2 s, const ulonglong2 sr, double q) {
     const double u = as_f(x), v = as_f(y);
@@ -278,6 +296,53 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // KI: 0 = exact, 1 = the unreduced integer schedule above (FASTI), 2 = FP64
 // schedule (q and nq carry the bit patterns of q and 1/q as doubles, the
 // tables are the FP64 ones; the last stage writes canonical integers).
+// The FP64 schedule's inverse stages P .. P_HI of a round: pairs of stages in
+// radix 4 (inv_bfly4_fp), a lone stage and the N^-1-scaled last stage in radix
+// 2.  Twiddle indexing as in inv_round.
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P, int P_HI>
+PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
+                          const ulonglong2* sptr, const ulonglong2* srptr, double q, double qinv) {
+    if constexpr (P <= P_HI) {
+        constexpr int E = 1 << LOG_E;
+        constexpr uint32_t N = 1u << LOG_N;
+        constexpr int r = P - G;
+        constexpr int h = 1 << r;
+        if constexpr (P == LOG_N - 1) {
+            const ulonglong2 s = *sptr, sr = *srptr;
+            static_for<0, E>([&](auto jt) {
+                constexpr int jj = decltype(jt)::value;
+                if constexpr (!(jj & h)) inv_last_bfly_fp(x[jj], x[jj + h], s, sr, q);
+            });
+        } else if constexpr (P + 1 <= P_HI && P + 1 < LOG_N - 1) {
+            // the first twiddle of each stage-P pair of groups sits at an even index
+            const ulonglong2* row0 = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
+            const ulonglong2* row1 = itw + (N - (N >> (P + 1))) + (((rank << LOG_M) + base) >> (P + 2));
+            static_for<0, (E >> (r + 2))>([&](auto kk) {
+                constexpr int k2 = decltype(kk)::value;
+                ulonglong2 wa, wb;
+                ldg_tw2(row0 + 2 * k2, wa, wb);
+                const ulonglong2 wc = __ldg(row1 + k2);
+                static_for<0, h>([&](auto ll) {
+                    constexpr int j0 = (k2 << (r + 2)) | decltype(ll)::value;
+                    inv_bfly4_fp(x[j0], x[j0 + h], x[j0 + 2 * h], x[j0 + 3 * h], wa, wb, wc, q, qinv);
+                });
+            });
+            inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P + 2, P_HI>(x, base, rank, itw, sptr, srptr, q, qinv);
+        } else {
+            const ulonglong2* row = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
+            static_for<0, (E >> (r + 1))>([&](auto kk) {
+                constexpr int k = decltype(kk)::value;
+                const ulonglong2 w = __ldg(row + k);
+                static_for<0, h>([&](auto ll) {
+                    constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
+                    inv_bfly_fp(x[jj], x[jj + h], w, q, qinv);
+                });
+            });
+            inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P + 1, P_HI>(x, base, rank, itw, sptr, srptr, q, qinv);
+        }
+    }
+}
+
 template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, int KI = 0>
 PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
                       const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq,
@@ -292,6 +357,10 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
     if constexpr (RED) {
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) x[jj] = reduce_full(x[jj], q, inv64, nq);
+    }
+    if constexpr (FP) {
+        inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P_LO, P_HI>(x, base, rank, itw, sptr, srptr, as_f(q), as_f(nq));
+        return;
     }
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
         constexpr int p = P_LO + decltype(it)::value;
