@@ -369,7 +369,7 @@ def run_gpu(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            import oracle as O  # the checker, timed as the CPU baseline only
+            import oracle as O  # the CPU oracle, timed here as the CPU baseline only
             moduli = O.ntt_primes(1 << 50, 2 * N, L)
             v, sample, thr = cpu_reference(moduli, seconds_target=args.cpu_seconds)
             cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}

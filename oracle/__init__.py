@@ -1,6 +1,6 @@
 """ctypes bindings for the CPU oracle (oracle/primus_oracle.c).
 
-TEST INFRASTRUCTURE ONLY.  This package is the checker: tests/, the smoke
+TEST INFRASTRUCTURE ONLY.  This package is the parity oracle: tests/, the smoke
 check in __graft_entry__.py and bench.py's CPU-baseline / reference arm import
 it.  The product package (primus_b200) never imports it.
 

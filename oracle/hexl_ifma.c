@@ -1,4 +1,4 @@
-/* CPU baseline, not a parity checker: the reference's fastest CPU transform
+/* CPU baseline, not the parity oracle: the reference's fastest CPU transform
  * path restated, i.e. the HEXL-style NTT with AVX-512 IFMA52 Harvey butterflies
  * that primus_ntt dispatches to when q < 2^50 and the host has avx512ifma
  * (primus_ntt/src/ntt/hexl/mod.rs:473-540; butterflies hexl/fwd.rs,

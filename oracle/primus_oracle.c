@@ -1,7 +1,7 @@
 /*
  * primus_oracle.c -- CPU restatement of the primus lattice-arithmetic path.
  *
- * TEST INFRASTRUCTURE ONLY (the checker).  Loaded by tests/, by the smoke
+ * TEST INFRASTRUCTURE ONLY (the parity oracle).  Loaded by tests/, by the smoke
  * check and by bench.py's CPU-baseline / reference arm; never by the product.
  *
  * Each function names the reference function it restates as

@@ -1,7 +1,7 @@
 /*
  * primus_oracle.h -- CPU restatement of the primus lattice-arithmetic path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/, the smoke
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity oracle: tests/, the smoke
  * check and bench.py's CPU-baseline / reference arm may load it; the product
  * library (primus_b200/libprimus_gpu.so) never links, loads or calls it.
  *

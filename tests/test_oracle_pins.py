@@ -1,4 +1,4 @@
-"""Pins the CPU oracle to the reference before it is used as the checker.
+"""Pins the CPU oracle to the reference before parity tests rely on it.
 
 The reference (Rust) cannot be built in this image, so the oracle is pinned by
 (a) the golden fixtures in tests/golden/ -- pure-Python big-integer values of
