@@ -113,6 +113,12 @@ typedef struct pg_ntt_table pg_ntt_table;
 int pg_ntt_table_create(uint32_t log_n, const uint64_t *h_moduli, uint32_t moduli_count,
                         pg_ntt_table **out);
 int pg_ntt_table_destroy(pg_ntt_table *table);
+/* A table over limbs [first, first + count) of `table` that shares its device
+ * arrays (DcrtTable::ntt_tables / iter, primus_ntt/src/dcrt/mod.rs: the
+ * per-prime tables of a DCRT table; count = 1 gives one prime's NttTable).
+ * The view keeps the parent's schedule setting and starts with default shapes;
+ * destroy it with pg_ntt_table_destroy before its parent. */
+int pg_ntt_table_view(const pg_ntt_table *table, uint32_t first, uint32_t count, pg_ntt_table **out);
 /* NTT kernel shapes.  Each ring degree has a default shape (rows per CTA,
  * elements per thread, cluster size) and, for N = 2^10 .. 2^16, alternatives
  * that compute identical values at different speed.  pg_ntt_autotune times

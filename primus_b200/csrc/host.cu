@@ -469,6 +469,10 @@ int pg_ntt_host_tables(uint32_t log_n, uint64_t q, uint64_t* root, uint64_t* inv
 
 static void free_table(pg_ntt_table* t) {
     if (!t) return;
+    if (t->view) {
+        delete t;
+        return;
+    }
     cudaFree(t->d_moduli);
     cudaFree(t->d_fwd);
     cudaFree(t->d_inv);
@@ -591,6 +595,40 @@ int pg_ntt_set_fp64(pg_ntt_table* t, int enable) {
 }
 
 int pg_ntt_fp64_enabled(const pg_ntt_table* t) { return t && t->fp64 ? 1 : 0; }
+
+int pg_ntt_table_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_table** out) {
+    if (!out) return set_error(PG_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!t) return set_error(PG_ERR_INVALID_ARGUMENT, "table is NULL");
+    if (count == 0 || first >= t->L || count > t->L - first)
+        return set_error(PG_ERR_INVALID_ARGUMENT, "limb range outside the table");
+    pg_ntt_table* v = new (std::nothrow) pg_ntt_table();
+    if (!v) return set_error(PG_ERR_OUT_OF_MEMORY, "table allocation failed");
+    const size_t n = t->n;
+    v->view = true;
+    v->log_n = t->log_n;
+    v->L = count;
+    v->n = n;
+    v->device = t->device;
+    v->moduli.assign(t->moduli.begin() + first, t->moduli.begin() + first + count);
+    v->host.assign(t->host.begin() + first, t->host.begin() + first + count);
+    v->d_moduli = t->d_moduli + first;
+    v->d_fwd = t->d_fwd + first * n;
+    v->d_inv = t->d_inv + first * n;
+    v->d_ordinal = t->d_ordinal + first * 2 * n;
+    v->d_inv_n = t->d_inv_n + first;
+    v->d_inv_last = t->d_inv_last + first;
+    v->d_barrett = t->d_barrett + first;
+    if (t->d_fwd_fp) {
+        v->d_fwd_fp = t->d_fwd_fp + first * n;
+        v->d_inv_fp = t->d_inv_fp + first * n;
+        v->d_inv_n_fp = t->d_inv_n_fp + first;
+        v->d_inv_last_fp = t->d_inv_last_fp + first;
+    }
+    v->fp64 = t->fp64;
+    *out = v;
+    return PG_OK;
+}
 
 int pg_ntt_table_destroy(pg_ntt_table* table) {
     free_table(table);

@@ -87,6 +87,7 @@ struct pg_ntt_table {
     uint32_t log_n = 0, L = 0;
     size_t n = 0;
     int device = 0;
+    bool view = false;                 // device arrays belong to another table
     std::vector<uint64_t> moduli;
     std::vector<pg::HostNttTable> host;
     uint64_t* d_moduli = nullptr;      // [L]

@@ -120,6 +120,20 @@ class DcrtTable:
             pass
 
     # ---- trait accessors
+    def ntt_tables(self) -> list:
+        """DcrtTable::ntt_tables: one single-prime table per limb, sharing this table's
+        device arrays (pg_ntt_table_view); they must not outlive this table."""
+        out = []
+        for l in range(len(self.moduli)):
+            h = C.c_void_p()
+            call("pg_ntt_table_view", self.h, l, 1, C.byref(h))
+            out.append(_TableView(h.value, self, self.log_n, [self.moduli[l]]))
+        return out
+
+    def iter(self):
+        """DcrtTable::iter: the per-prime tables in limb order."""
+        return iter(self.ntt_tables())
+
     def poly_length(self) -> int:
         return self.n
 
@@ -255,6 +269,16 @@ class DcrtTable:
 
     def butterfly_mul_factor(self, a, s, w, wq, b, polys, stream=None):
         call("pg_dcrt_butterfly_mul_factor", self.h, a.ptr, s.ptr, w.ptr, wq.ptr, b.ptr, polys, _sh(stream))
+
+
+class _TableView(DcrtTable):
+    """A table over some limbs of another table (pg_ntt_table_view): the same
+    methods, the parent's device arrays; keeps its parent alive."""
+
+    def __init__(self, h, parent, log_n, moduli):
+        self.h, self.parent, self.log_n, self.moduli = h, parent, log_n, list(moduli)
+        self.n = 1 << log_n
+        self.L = len(self.moduli)
 
 
 class NttTable(DcrtTable):

@@ -266,3 +266,34 @@ def test_full_size_fused_round_trip_repeatable(gpu):
             assert np.array_equal(got[:per], exp)
         else:
             assert np.array_equal(got, first), f"rep {rep} differs"
+
+
+def test_ntt_tables_views(gpu):
+    """DcrtTable::ntt_tables / iter: per-prime views over the DCRT table's device arrays
+    (pg_ntt_table_view) transform like single-prime tables of the same primes."""
+    log_n, L = 12, 3
+    n = 1 << log_n
+    moduli = primes_for(log_n, L)
+    tab = gpu.DcrtTable(log_n, moduli)
+    views = tab.ntt_tables()
+    assert [v.moduli for v in views] == [[q] for q in moduli]
+    assert [v.moduli for v in tab.iter()] == [[q] for q in moduli]
+    x = lazy_inputs(moduli, n, 2, 77, 4)
+    for l, (v, q) in enumerate(zip(views, moduli)):
+        ref = O.NttTable(log_n, q)
+        rows = np.ascontiguousarray(x[:, l, :])
+        d = gpu.DeviceBuffer.from_numpy(rows)
+        v.forward(d, 2)
+        assert np.array_equal(d.numpy(rows.shape), np.stack([ref.forward(r.copy()) for r in rows]))
+        slice_ = rows[0] % np.uint64(q)
+        v.transform_slice(slice_)
+        assert np.array_equal(slice_, ref.forward((rows[0] % np.uint64(q)).copy()))
+    from primus_b200 import _native as nat
+    import ctypes as C
+    h = C.c_void_p()
+    assert nat.lib().pg_ntt_table_view(tab.h, L, 1, C.byref(h)) == nat.PG_ERR_INVALID_ARGUMENT
+    assert nat.lib().pg_ntt_table_view(tab.h, 1, L, C.byref(h)) == nat.PG_ERR_INVALID_ARGUMENT
+    del views
+    d = gpu.DeviceBuffer.from_numpy(x)
+    tab.forward(d, 2)  # the parent keeps working after its views are gone
+    assert np.array_equal(d.numpy(x.shape), O.DcrtTable(log_n, moduli).forward(x).reshape(x.shape))
