@@ -541,7 +541,8 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
     if (e == cudaSuccess)
         e = cudaMemcpy(t->d_inv_last, invlast.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->d_barrett, bar.data(), L * sizeof(Barrett), cudaMemcpyHostToDevice);
-    // FP64-schedule copies: (w, w / q) as doubles (exact values, correctly rounded quotients)
+    // FP64-schedule copies: w / q correctly rounded (forward and inverse tables; the
+    // kernels recover w = rint(wq q)), (w, w / q) pairs for the two N^-1 factors
     uint64_t maxq = 0;
     for (uint64_t m : t->moduli) maxq = m > maxq ? m : maxq;
     if (e == cudaSuccess && maxq < (1ull << 50)) {
@@ -553,24 +554,25 @@ int pg_ntt_table_create(uint32_t log_n, const uint64_t* h_moduli, uint32_t modul
             std::memcpy(&b, &wq, 8);
             return make_ulonglong2(a, b);
         };
-        std::vector<ulonglong2> ffwd(L * n), finv(L * n), finvn(L), finvlast(L);
+        std::vector<double> ffwd(L * n), finv(L * n);
+        std::vector<ulonglong2> finvn(L), finvlast(L);
         for (size_t l = 0; l < L; ++l) {
             const uint64_t q = t->moduli[l];
             for (size_t i = 0; i < n; ++i) {
-                ffwd[l * n + i] = fp(fwd[l * n + i], q);
-                finv[l * n + i] = fp(inv[l * n + i], q);
+                ffwd[l * n + i] = (double)fwd[l * n + i].x / (double)q;
+                finv[l * n + i] = (double)inv[l * n + i].x / (double)q;
             }
             finvn[l] = fp(invn[l], q);
             finvlast[l] = fp(invlast[l], q);
         }
-        e = cudaMalloc(&t->d_fwd_fp, L * n * sizeof(ulonglong2));
-        if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_fp, L * n * sizeof(ulonglong2));
+        e = cudaMalloc(&t->d_fwd_fp, L * n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_fp, L * n * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_n_fp, L * sizeof(ulonglong2));
         if (e == cudaSuccess) e = cudaMalloc(&t->d_inv_last_fp, L * sizeof(ulonglong2));
         if (e == cudaSuccess)
-            e = cudaMemcpy(t->d_fwd_fp, ffwd.data(), L * n * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+            e = cudaMemcpy(t->d_fwd_fp, ffwd.data(), L * n * sizeof(double), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
-            e = cudaMemcpy(t->d_inv_fp, finv.data(), L * n * sizeof(ulonglong2), cudaMemcpyHostToDevice);
+            e = cudaMemcpy(t->d_inv_fp, finv.data(), L * n * sizeof(double), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
             e = cudaMemcpy(t->d_inv_n_fp, finvn.data(), L * sizeof(ulonglong2), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)

@@ -97,10 +97,12 @@ struct pg_ntt_table {
     ulonglong2* d_inv_n = nullptr;     // [L] N^-1
     ulonglong2* d_inv_last = nullptr;  // [L] inv_root_powers[N-1] * N^-1
     pg::Barrett* d_barrett = nullptr;  // [L]
-    // the four twiddle tables above with (w, w / q) as doubles, for the FP64
-    // schedule; allocated when every modulus is below 2^50
-    ulonglong2* d_fwd_fp = nullptr;
-    ulonglong2* d_inv_fp = nullptr;
+    // FP64-schedule copies of the four twiddle tables, allocated when every
+    // modulus is below 2^50: the forward and inverse tables as w / q only (a
+    // double per twiddle, w = rint(wq q) recovered in the kernels), the two
+    // N^-1 factors as (w, w / q) pairs of doubles
+    double* d_fwd_fp = nullptr;
+    double* d_inv_fp = nullptr;
     ulonglong2* d_inv_n_fp = nullptr;
     ulonglong2* d_inv_last_fp = nullptr;
     int fp64 = 0;                       // FP64 schedule in use (tables present and not switched off)
@@ -129,9 +131,9 @@ struct NttArgs {
     const uint64_t* plain;
     const uint64_t* plain_q;
     const Barrett* bar;
-    // FP64-schedule twiddles: the same tables with (w, w / q) as doubles
-    const ulonglong2* fwd_fp;
-    const ulonglong2* inv_fp;
+    // FP64-schedule twiddles: w / q per twiddle (fwd, inv), (w, w / q) pairs (N^-1 factors)
+    const double* fwd_fp;
+    const double* inv_fp;
     const ulonglong2* inv_n_fp;
     const ulonglong2* inv_last_fp;
     const RowDesc* desc;  // NULL: rows are [polys][L][N] at data

@@ -134,8 +134,8 @@ PG_DEV uint64_t canon4(uint64_t v, uint64_t q, uint64_t q2) {
 // residues travel as doubles holding signed integers and every operation
 // below is exact (each result is an integer of magnitude below 2^53, which
 // round-to-nearest reproduces).  Register and shared-memory words keep the
-// double's bit pattern.  Twiddle tables hold (w, wq) with wq = w / q
-// correctly rounded (wq < 1 because w < q).
+// double's bit pattern.  Twiddle tables hold wq = w / q correctly rounded
+// (wq < 1 because w < q), 8 bytes per twiddle; tw_fp recovers w from it.
 //
 // fmulmod(y, w, wq, q) = w y mod q in (-0.75 q, 0.75 q) for |y| < 2^51:
 //   t  = fma(y, wq, 1.5*2^52) rounds y*wq to the nearest integer (|y wq| < 2^51
@@ -172,6 +172,14 @@ PG_DEV double freduce(double x, double q, double qinv) {
 
 // x in (-q, q) -> [0, q)
 PG_DEV double fcanon(double x, double q) { return x < 0.0 ? __dadd_rn(x, q) : x; }
+
+// table entry wq = w / q (correctly rounded) -> (w, wq) as double bit patterns.
+// |wq - w/q| <= 2^-53 so |wq q - w| <= q 2^-53 < 1/8 for q < 2^50: rounding
+// wq q to the nearest integer (by the 1.5 * 2^52 constant) gives w exactly.
+PG_DEV ulonglong2 tw_fp(double wq, double q) {
+    const double w = __dsub_rn(__fma_rn(wq, q, kMagic52), kMagic52);
+    return make_ulonglong2(as_u(w), as_u(wq));
+}
 
 // Cooley-Tukey forward butterfly: (u + w y, u - w y).  RU reduces u first.
 // Inputs below 2q + 2 in magnitude; with u reduced at least every other stage
@@ -235,15 +243,30 @@ PG_DEV void ldg_tw2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
     b = make_ulonglong2(b0, b1);
 }
 
+// FP64 tables: 2 (16-byte aligned) or 4 (32-byte aligned) consecutive quotients
+PG_DEV void ldg_f2(const double* p, double& a, double& b) {
+    asm("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "l"(p));
+}
+PG_DEV void ldg_f4(const double* p, double (&w)[4]) {
+    uint64_t b0, b1, b2, b3;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(b0), "=l"(b1), "=l"(b2), "=l"(b3) : "l"(p));
+    w[0] = as_f(b0);
+    w[1] = as_f(b1);
+    w[2] = as_f(b2);
+    w[3] = as_f(b3);
+}
+
 // One forward round over register group x (x[jj] is local index base + (jj << G)
 // of a 2^LOG_M block).  Stage bits P_HI down to P_LO; stage bit p is block stage
 // sp = LOG_M-1-p and uses tw[(tw_base << sp) + (i >> (p+1))], tw_base = C + rank
 // for a cluster block (1 for a whole row).  When a stage needs two or more
-// twiddles their first index is even, so they are fetched in 32-byte pairs.
+// twiddles their first index is a multiple of their count, so they are fetched
+// in 32-byte pieces (two integer or four FP64 twiddles).
 // K: 0 = exact schedule, 1 = fast integer schedule, 2 = FP64 schedule (then q2
-// and nq carry the bit patterns of q and 1/q as doubles and tw is the FP64 table)
-template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, int K>
-PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const ulonglong2* __restrict__ tw,
+// and nq carry the bit patterns of q and 1/q as doubles and tw is the FP64
+// quotient table, TW = double)
+template <int LOG_M, int LOG_E, int G, int P_HI, int P_LO, int K, typename TW>
+PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base, const TW* __restrict__ tw,
                       uint64_t q2, uint64_t nq) {
     constexpr int E = 1 << LOG_E;
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
@@ -252,7 +275,7 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
         constexpr int half = 1 << r;
         constexpr int sp = LOG_M - 1 - p;
         constexpr int nk = E >> (r + 1);
-        const ulonglong2* row = tw + (tw_base << sp) + (base >> (p + 1));
+        const TW* row = tw + (tw_base << sp) + (base >> (p + 1));
         auto bfly_k = [&](auto kk, const ulonglong2 w) {
             constexpr int k = decltype(kk)::value;
             static_for<0, half>([&](auto ll) {
@@ -265,7 +288,27 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
                     fwd_bfly(x[jj], x[jj + half], w, q2, nq);
             });
         };
-        if constexpr (nk == 1) {
+        if constexpr (K == 2) {
+            const double q = as_f(q2);
+            if constexpr (nk == 1) {
+                bfly_k(IC<0>{}, tw_fp(__ldg(row), q));
+            } else if constexpr (nk == 2) {
+                double w0, w1;
+                ldg_f2(row, w0, w1);
+                bfly_k(IC<0>{}, tw_fp(w0, q));
+                bfly_k(IC<1>{}, tw_fp(w1, q));
+            } else {
+                static_for<0, nk / 4>([&](auto kp) {
+                    constexpr int k = 4 * decltype(kp)::value;
+                    double w[4];
+                    ldg_f4(row + k, w);
+                    bfly_k(IC<k>{}, tw_fp(w[0], q));
+                    bfly_k(IC<k + 1>{}, tw_fp(w[1], q));
+                    bfly_k(IC<k + 2>{}, tw_fp(w[2], q));
+                    bfly_k(IC<k + 3>{}, tw_fp(w[3], q));
+                });
+            }
+        } else if constexpr (nk == 1) {
             bfly_k(IC<0>{}, __ldg(row));
         } else {
             static_for<0, nk / 2>([&](auto kp) {
@@ -300,7 +343,7 @@ PG_DEV void fwd_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t tw_base
 // radix 4 (inv_bfly4_fp), a lone stage and the N^-1-scaled last stage in radix
 // 2.  Twiddle indexing as in inv_round.
 template <int LOG_N, int LOG_M, int LOG_E, int G, int P, int P_HI>
-PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
+PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const double* __restrict__ itw,
                           const ulonglong2* sptr, const ulonglong2* srptr, double q, double qinv) {
     if constexpr (P <= P_HI) {
         constexpr int E = 1 << LOG_E;
@@ -315,13 +358,13 @@ PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t ran
             });
         } else if constexpr (P + 1 <= P_HI && P + 1 < LOG_N - 1) {
             // the first twiddle of each stage-P pair of groups sits at an even index
-            const ulonglong2* row0 = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
-            const ulonglong2* row1 = itw + (N - (N >> (P + 1))) + (((rank << LOG_M) + base) >> (P + 2));
+            const double* row0 = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
+            const double* row1 = itw + (N - (N >> (P + 1))) + (((rank << LOG_M) + base) >> (P + 2));
             static_for<0, (E >> (r + 2))>([&](auto kk) {
                 constexpr int k2 = decltype(kk)::value;
-                ulonglong2 wa, wb;
-                ldg_tw2(row0 + 2 * k2, wa, wb);
-                const ulonglong2 wc = __ldg(row1 + k2);
+                double qa, qb;
+                ldg_f2(row0 + 2 * k2, qa, qb);
+                const ulonglong2 wa = tw_fp(qa, q), wb = tw_fp(qb, q), wc = tw_fp(__ldg(row1 + k2), q);
                 static_for<0, h>([&](auto ll) {
                     constexpr int j0 = (k2 << (r + 2)) | decltype(ll)::value;
                     inv_bfly4_fp(x[j0], x[j0 + h], x[j0 + 2 * h], x[j0 + 3 * h], wa, wb, wc, q, qinv);
@@ -329,10 +372,10 @@ PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t ran
             });
             inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P + 2, P_HI>(x, base, rank, itw, sptr, srptr, q, qinv);
         } else {
-            const ulonglong2* row = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
+            const double* row = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
             static_for<0, (E >> (r + 1))>([&](auto kk) {
                 constexpr int k = decltype(kk)::value;
-                const ulonglong2 w = __ldg(row + k);
+                const ulonglong2 w = tw_fp(__ldg(row + k), q);
                 static_for<0, h>([&](auto ll) {
                     constexpr int jj = (k << (r + 1)) | decltype(ll)::value;
                     inv_bfly_fp(x[jj], x[jj + h], w, q, qinv);
@@ -343,8 +386,8 @@ PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t ran
     }
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, int KI = 0>
-PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const ulonglong2* __restrict__ itw,
+template <int LOG_N, int LOG_M, int LOG_E, int G, int P_LO, int P_HI, int KI = 0, typename TW = ulonglong2>
+PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, const TW* __restrict__ itw,
                       const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q, uint64_t nq,
                       uint64_t inv64 = 0) {
     constexpr bool FASTI = KI == 1, FP = KI == 2;
@@ -360,8 +403,7 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
     }
     if constexpr (FP) {
         inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P_LO, P_HI>(x, base, rank, itw, sptr, srptr, as_f(q), as_f(nq));
-        return;
-    }
+    } else {
     static_for<0, P_HI - P_LO + 1>([&](auto it) {
         constexpr int p = P_LO + decltype(it)::value;
         constexpr int r = p - G;
@@ -407,6 +449,7 @@ PG_DEV void inv_round(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t rank, c
             }
         }
     });
+    }
 }
 
 template <int LOG_E, int G>
@@ -439,9 +482,9 @@ struct FwdRounds {
 // Runs forward rounds R..last; x holds round R-1's group on entry (stored to
 // smem first).  On exit x holds the last round's group (G = 0: E contiguous
 // elements at tid*E).
-template <int LOG_M, int TOP, int LOG_E, int R, int FAST>
+template <int LOG_M, int TOP, int LOG_E, int R, int FAST, typename TW>
 PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t tw_base,
-                     const ulonglong2* __restrict__ tw, uint64_t q2, uint64_t nq) {
+                     const TW* __restrict__ tw, uint64_t q2, uint64_t nq) {
     if constexpr (R < FwdRounds<TOP, LOG_E, 0>::COUNT) {
         using Cur = FwdRounds<TOP, LOG_E, R>;
         using Prev = FwdRounds<TOP, LOG_E, R - 1>;
@@ -465,9 +508,9 @@ struct InvRounds {
 
 // Runs inverse rounds R .. R_END-1; x holds round R-1's group on entry
 // (R >= 1) and is stored to smem first.  On exit x holds round R_END-1's group.
-template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END, int FASTI = 0>
+template <int LOG_N, int LOG_M, int TOP, int LOG_E, int R, int R_END, int FASTI = 0, typename TW = ulonglong2>
 PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint32_t rank,
-                      const ulonglong2* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
+                      const TW* __restrict__ itw, const ulonglong2* sptr, const ulonglong2* srptr, uint64_t q,
                       uint64_t nq, uint64_t inv64 = 0) {
     if constexpr (R < R_END) {
         using Cur = InvRounds<TOP, LOG_E, R>;
@@ -490,6 +533,16 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
 //   kSchedFp64     both directions on the FP64 pipe (fwd_bfly_fp / inv_bfly_fp):
 //                  every q < 2^50, canonical (non-lazy) forward outputs
 constexpr int kSchedExact = 0, kSchedFastFwd = 1, kSchedFastBoth = 2, kSchedFp64 = 3;
+
+// twiddle tables of a schedule: (w, w') pairs, or the FP64 quotient tables
+template <bool FP>
+PG_DEV auto fwd_table(const NttArgs& a) {
+    if constexpr (FP) return a.fwd_fp; else return a.fwd;
+}
+template <bool FP>
+PG_DEV auto inv_table(const NttArgs& a) {
+    if constexpr (FP) return a.inv_fp; else return a.inv;
+}
 
 // per-row constants of the FP64 schedule: q and 1/q (correctly rounded)
 struct FpMod {
@@ -539,7 +592,7 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     uint64_t x[E];
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
-        const ulonglong2* tw = (FP ? a.fwd_fp : a.fwd) + (size_t)limb * N;
+        const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         using R0 = FwdRounds<LOG_N, LOG_E, 0>;
         // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
 #pragma unroll
@@ -590,7 +643,7 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     }
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
-        const ulonglong2* itw = (FP ? a.inv_fp : a.inv) + (size_t)limb * N;
+        const auto* itw = inv_table<FP>(a) + (size_t)limb * N;
         const ulonglong2* sptr = (FP ? a.inv_n_fp : a.inv_n) + limb;
         const ulonglong2* srptr = (FP ? a.inv_last_fp : a.inv_last) + limb;
         const uint64_t iA = FP ? as_u(fm.q) : q, iB = FP ? as_u(fm.qinv) : nq;
@@ -695,7 +748,7 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         const uint64_t q2 = q << 1;
         // the rounds' modulus words: (2q, -q) on the integer schedules, (q, 1/q) as doubles on FP64
         const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
-        const ulonglong2* tw = (FP ? a.fwd_fp : a.fwd) + (size_t)limb * N;
+        const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         // matched by the wait before the first remote store; relaxed is enough
         // because this CTA has not touched shared memory yet
         cluster_arrive_relaxed();
@@ -755,7 +808,7 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
     }
     // ---------------- inverse
     if constexpr (MODE != MODE_FWD) {
-        const ulonglong2* itw = (FP ? a.inv_fp : a.inv) + (size_t)limb * N;
+        const auto* itw = inv_table<FP>(a) + (size_t)limb * N;
         const uint64_t iA = FP ? as_u(fm.q) : q, iB = FP ? as_u(fm.qinv) : nq;
         using I0 = InvRounds<TOP, LOG_E, 0>;
         using ILast = InvRounds<TOP, LOG_E, I0::COUNT - 1>;
