@@ -360,16 +360,30 @@ PG_DEV void inv_stages_fp(uint64_t (&x)[1 << LOG_E], uint32_t base, uint32_t ran
             // the first twiddle of each stage-P pair of groups sits at an even index
             const double* row0 = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
             const double* row1 = itw + (N - (N >> (P + 1))) + (((rank << LOG_M) + base) >> (P + 2));
-            static_for<0, (E >> (r + 2))>([&](auto kk) {
+            constexpr int n4 = E >> (r + 2);  // radix-4 groups of this stage pair
+            auto bfly4_k = [&](auto kk, const ulonglong2 wa, const ulonglong2 wb, const ulonglong2 wc) {
                 constexpr int k2 = decltype(kk)::value;
-                double qa, qb;
-                ldg_f2(row0 + 2 * k2, qa, qb);
-                const ulonglong2 wa = tw_fp(qa, q), wb = tw_fp(qb, q), wc = tw_fp(__ldg(row1 + k2), q);
                 static_for<0, h>([&](auto ll) {
                     constexpr int j0 = (k2 << (r + 2)) | decltype(ll)::value;
                     inv_bfly4_fp(x[j0], x[j0 + h], x[j0 + 2 * h], x[j0 + 3 * h], wa, wb, wc, q, qinv);
                 });
-            });
+            };
+            if constexpr (n4 == 1) {
+                double qa, qb;
+                ldg_f2(row0, qa, qb);
+                bfly4_k(IC<0>{}, tw_fp(qa, q), tw_fp(qb, q), tw_fp(__ldg(row1), q));
+            } else {
+                // with two or more groups the stage-P indices start at a multiple
+                // of 4 and the stage-(P+1) ones at a multiple of 2
+                static_for<0, n4 / 2>([&](auto kp) {
+                    constexpr int k2 = 2 * decltype(kp)::value;
+                    double wq[4], c0, c1;
+                    ldg_f4(row0 + 2 * k2, wq);
+                    ldg_f2(row1 + k2, c0, c1);
+                    bfly4_k(IC<k2>{}, tw_fp(wq[0], q), tw_fp(wq[1], q), tw_fp(c0, q));
+                    bfly4_k(IC<k2 + 1>{}, tw_fp(wq[2], q), tw_fp(wq[3], q), tw_fp(c1, q));
+                });
+            }
             inv_stages_fp<LOG_N, LOG_M, LOG_E, G, P + 2, P_HI>(x, base, rank, itw, sptr, srptr, q, qinv);
         } else {
             const double* row = itw + (N - (N >> P)) + (((rank << LOG_M) + base) >> (P + 1));
