@@ -6,7 +6,7 @@
  * layer: its boundary is a set of traits and inherent methods.  Each entry
  * point below names the reference item it replaces (crate/src/file.rs:line).
  * A Rust `primus_gpu` crate binds these symbols with `extern "C"` and
- * implements `NttTable` / `DcrtTable` on top of them (INTEGRATION.md).
+ * implements `NttTable` / `DcrtTable` on top of them.
  *
  * Conventions
  *  - Every function returns an int status (PG_OK == 0); none aborts.  The
@@ -466,10 +466,14 @@ int pg_ggsw_pk_encrypt_monomial(const pg_glwe_encryptor *encryptor, const pg_gad
 /* pg_ext_product for callers that cannot allocate device memory when they
  * call (hosts holding only device pointers owned by another runtime, serving
  * processes that reserve HBM at start-up and forbid later allocations).  No
- * counterpart in the reference: it exists for this library's C callers.  The
- * scratch is a fixed 32 MiB device array inside the library, held by every GPU
- * that loads it until the process exits; batches needing more are rejected
- * with PG_ERR_UNSUPPORTED and a message giving the largest batch of that shape.
+ * counterpart in the reference: it exists for this library's C callers.
+ * Shapes the fused external-product kernel takes (k = 1, one prime,
+ * single-word gadget values, N = 2^10..2^12, batch >= 64, 16-byte aligned
+ * key and output) need no scratch and run there, up to 2^31 - 1 ciphertexts
+ * per call.  Every other shape keeps its scratch in a fixed 32 MiB device
+ * array inside the library, held by every GPU that loads it until the process
+ * exits; a batch needing more is refused before any launch with
+ * PG_ERR_UNSUPPORTED and a message giving the largest batch of that shape.
  * The first call on each device looks up the array's device address, so make
  * that first call before any stream capture.  No scratch word needs to start
  * at zero, but every call shares the array: calls whose work overlaps on the

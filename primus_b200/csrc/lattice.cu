@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
+#include <string>
 
 #include "internal.hpp"
 
@@ -66,8 +67,8 @@ struct MacArgs {
 // coefficient x); lanes run over consecutive coefficients (coalesced).  Each
 // digit element is loaded once for both output polys of the pair and each key
 // element once for the whole chunk, so a batch reads the digits once per pair
-// of output polys and the key ceil(B / kMacChunk) times.  Grid: x over the
-// coefficients of a poly (32-bit index), y over (chunk, output pair).
+// of output polys and the key ceil(B / kMacChunk) times.  Grid: x over
+// (chunk, output pair), y over 256-coefficient tiles (32-bit index).
 constexpr uint32_t kMacChunk = 2;
 constexpr uint32_t kMacOut = 2;
 
@@ -194,12 +195,27 @@ int check_compat(const pg_ntt_table* t, const pg_gadget_basis* g) {
     return PG_OK;
 }
 
-// workspace: BigUint values [P][N][W] + lifted digits [P][d][L][N] (+ extra)
+// workspace: BigUint values [P][N][W] + lifted digits [P][d][L][N] (+ extra).
+// Every product and sum is overflow-checked: a size that does not fit size_t
+// returns SIZE_MAX, which no workspace, pool or fixed array satisfies, so a
+// huge batch is refused on the host instead of wrapping to a small size.
 size_t ws_bytes(const pg_ntt_table* t, const pg_gadget_basis* g, size_t polys, size_t extra_words) {
     const pg_rns_base* b = gadget_base(g);
-    const size_t big = polys * t->n * rns_W(b);
-    const size_t dig = polys * gadget_d(g) * (size_t)t->L * t->n;
-    return (big + dig + extra_words) * sizeof(uint64_t) + 256;
+    size_t per = 0, words = 0, bytes = 0;
+    // words per poly: N * W (BigUint values) + d * L * N (lifted digit rows);
+    // (N <= 2^16, W <= 64 limbs, d <= 4096 digits, L <= 64 moduli: below 2^35)
+    const size_t per_poly = t->n * rns_W(b) + (size_t)gadget_d(g) * t->L * t->n;
+    if (__builtin_mul_overflow(polys, per_poly, &per)) return SIZE_MAX;
+    if (__builtin_add_overflow(per, extra_words, &words)) return SIZE_MAX;
+    if (__builtin_mul_overflow(words, sizeof(uint64_t), &bytes)) return SIZE_MAX;
+    if (__builtin_add_overflow(bytes, (size_t)256, &bytes)) return SIZE_MAX;
+    return bytes;
+}
+
+// checked a * b for the callers' extra-word counts (SIZE_MAX on overflow)
+size_t mul_sat(size_t a, size_t b) {
+    size_t r = 0;
+    return __builtin_mul_overflow(a, b, &r) ? SIZE_MAX : r;
 }
 
 struct Workspace {
@@ -312,7 +328,7 @@ int ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, con
         return launch_ext_fused(t, gw, d_in, d_ggsw, d_out, batch, out_coeff, st);
     const size_t polys = batch * (k + 1);
     Workspace w;
-    int rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, 0), st);
+    int rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, mul_sat(batch, k + 1), 0), st);
     if (rc) return rc;
     uint64_t* dig = nullptr;
     rc = digits_pipeline(t, g, d_in, true, polys, k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)w.ptr, &dig, st);
@@ -364,7 +380,7 @@ extern "C" {
 
 size_t pg_ext_product_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, size_t batch) {
     if (!t || !g) return 0;
-    return ws_bytes(t, g, batch * (k + 1), 0);
+    return ws_bytes(t, g, mul_sat(batch, k + 1), 0);
 }
 
 int pg_ext_product(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
@@ -422,7 +438,7 @@ size_t pg_key_switch_workspace_size(const pg_ntt_table* t, const pg_gadget_basis
                                     size_t batch) {
     (void)k_out;
     if (!t || !g) return 0;
-    return ws_bytes(t, g, batch * k_in, batch * (size_t)t->L * t->n);
+    return ws_bytes(t, g, mul_sat(batch, k_in), mul_sat(batch, (size_t)t->L * t->n));
 }
 
 int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in, uint32_t k_out,
@@ -437,7 +453,7 @@ int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in
     const size_t LN = (size_t)t->L * t->n;
     const size_t polys = batch * k_in;
     Workspace w;
-    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, polys, batch * LN), st);
+    rc = get_workspace(w, d_ws, ws_size, ws_bytes(t, g, mul_sat(batch, k_in), mul_sat(batch, LN)), st);
     if (rc) return rc;
     uint64_t* ws = (uint64_t*)w.ptr;
     uint64_t* dig = nullptr;
@@ -456,7 +472,7 @@ int pg_key_switch(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k_in
 size_t pg_glwe_automorphism_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k,
                                            size_t batch) {
     if (!t || !g) return 0;
-    return ws_bytes(t, g, batch * k, batch * (k + 1) * (size_t)t->L * t->n);
+    return ws_bytes(t, g, mul_sat(batch, k), mul_sat(batch, (k + 1) * (size_t)t->L * t->n));
 }
 
 // DcrtGlweAutoKey::automorphism_inplace (primus_fhe_core/src/automorphism/glwe/dcrt.rs:269-331):
@@ -493,28 +509,45 @@ int pg_glwe_automorphism(const pg_ntt_table* t, const pg_gadget_basis* g, uint32
     return launch_mac(t, gadget_d(g), d_out, nullptr, pb, d_key, dig, batch, k, k + 1, 1, st);
 }
 
-// Same computation and outputs as pg_ext_product, with its scratch in the
-// library's fixed device array instead of caller or runtime allocations.
+// Same computation and outputs as pg_ext_product, without any device
+// allocation.  The shapes the fused kernel takes (k = 1, one prime, single-word
+// gadget values, N = 2^10..2^12, at least kExtFusedMinBatch ciphertexts) run
+// there and use no scratch at all, so their batch is bounded only by one
+// launch; every other shape runs the pipeline with its scratch in the
+// library's fixed device array and is refused, before anything is launched,
+// when that array is too small.
 int pg_ext_product_noalloc(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, const uint64_t* d_in,
                            const uint64_t* d_ggsw, uint64_t* d_out, size_t batch, void* stream) {
     int rc = check_compat(t, g);
     if (rc) return rc;
     if (batch == 0) return PG_OK;
-    if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
-    const size_t need = ws_bytes(t, g, batch * (k + 1), 0);
-    if (need > kNoAllocScratchBytes) {
-        const size_t per = ws_bytes(t, g, (size_t)(k + 1), 0);
-        char buf[256];
-        snprintf(buf, sizeof buf,
-                 "pg_ext_product_noalloc: this batch needs %zu bytes of scratch, above the fixed %zu bytes; "
-                 "submit at most %zu ciphertexts of this shape per call",
-                 need, kNoAllocScratchBytes, per ? kNoAllocScratchBytes / per : (size_t)0);
-        return set_error(PG_ERR_UNSUPPORTED, buf);
+    cudaStream_t st = (cudaStream_t)stream;
+    GadgetWord gw;
+    const bool aligned = ((uintptr_t)d_ggsw % 16 == 0) && ((uintptr_t)d_out % 16 == 0);
+    const bool fused = batch >= kExtFusedMinBatch && aligned && gadget_word(g, &gw) && ext_fused_eligible(t, gw, k);
+    if (!fused) {
+        // the size check comes first, so that an oversized batch is refused on
+        // the host whatever the buffers are
+        const size_t need = ws_bytes(t, g, mul_sat(batch, k + 1), 0);
+        if (need > kNoAllocScratchBytes) {
+            // ws_bytes adds one fixed 256-byte pad per call: the largest batch b
+            // has b * (per - 256) + 256 <= the array
+            const size_t per = ws_bytes(t, g, (size_t)(k + 1), 0);
+            const size_t max_batch = per > 256 ? (kNoAllocScratchBytes - 256) / (per - 256) : 0;
+            char buf[320];
+            snprintf(buf, sizeof buf,
+                     "pg_ext_product_noalloc: this batch needs %s bytes of scratch, above the fixed %zu bytes; "
+                     "submit at most %zu ciphertexts of this shape per call",
+                     need == SIZE_MAX ? "more than SIZE_MAX" : std::to_string(need).c_str(), kNoAllocScratchBytes,
+                     max_batch);
+            return set_error(PG_ERR_UNSUPPORTED, buf);
+        }
     }
+    if (!d_in || !d_ggsw || !d_out) return set_error(PG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (fused) return launch_ext_fused(t, gw, d_in, d_ggsw, d_out, batch, false, st);
     void* ws = nullptr;
     rc = noalloc_scratch(&ws);
     if (rc) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
     uint64_t* dig = nullptr;
     rc = digits_pipeline(t, g, d_in, true, batch * (k + 1), k + 1, (size_t)(k + 1) * t->L * t->n, (uint64_t*)ws,
                          &dig, st);
@@ -549,7 +582,11 @@ extern "C" {
 
 size_t pg_glwe_trace_workspace_size(const pg_ntt_table* t, const pg_gadget_basis* g, uint32_t k, size_t batch) {
     if (!t || !g) return 0;
-    return round256(batch * (k + 1) * (size_t)t->L * t->n * 8) + pg_glwe_automorphism_workspace_size(t, g, k, batch);
+    const size_t sums = mul_sat(mul_sat(batch, (k + 1) * (size_t)t->L * t->n), sizeof(uint64_t));
+    const size_t autos = pg_glwe_automorphism_workspace_size(t, g, k, batch);
+    // saturate: a batch whose size does not fit size_t gets SIZE_MAX, which no workspace satisfies
+    if (sums > SIZE_MAX / 2 || autos > SIZE_MAX / 2) return SIZE_MAX;
+    return round256(sums) + autos;
 }
 
 // DcrtGlweTraceKey::trace_inplace (primus_fhe_core/src/trace/glwe/dcrt.rs:84-108):
