@@ -212,6 +212,62 @@ def cpu_reference(moduli, seconds_target=12.0, threads=None, path=None):
                                   f"trip x {reps}, {dt:.2f} s", threads
 
 
+class RowCheck:
+    """Checks the bench's own outputs against the oracle after the timed region.
+
+    Every leg of the bench applies the same map to the batch in place (forward
+    NTT, product with the NTT-domain plaintext, inverse NTT), so after R round
+    trips row r holds RT^R(x_r).  Four rows (one limb each of four polys) are
+    regenerated from the seed on the host and carried forward by the oracle
+    (UintNttTable transforms, primus_ntt/src/ntt/primitive.rs:211-296, and the
+    pointwise product); `check` compares the device's rows with them after any
+    number of round trips.  It runs outside every timed region."""
+
+    def __init__(self, moduli, seed, threads):
+        import oracle as O
+        self.O = O
+        self.polys = sorted({0, POLYS // 3, (2 * POLYS) // 3, POLYS - 1})
+        self.limbs = [(7 * i + 3) % L for i in range(len(self.polys))]
+        self.moduli = [moduli[l] for l in self.limbs]
+        self.ref = O.DcrtTable(LOG_N, self.moduli)
+        plain = O.DcrtTable(LOG_N, moduli).forward(O.uniform_rns(SEED + 7, 0, moduli, N), threads=threads)
+        self.plain = np.stack([plain.reshape(L, N)[l] for l in self.limbs])
+        self.state = np.stack([O.uniform(seed, p * L + l, moduli[l], N) for p, l in zip(self.polys, self.limbs)])
+        self.rounds = 0
+        self.threads = threads
+        self.results = []
+
+    def advance(self, rounds):
+        while self.rounds < rounds:
+            self.state = self.ref.polymul_roundtrip(self.state, self.plain, threads=self.threads).reshape(
+                self.state.shape)
+            self.rounds += 1
+
+    def rows_of(self, read_row):
+        return np.stack([read_row(p * L + l) for p, l in zip(self.polys, self.limbs)])
+
+    def check(self, name, rounds, read_row):
+        self.advance(rounds)
+        ok = bool(np.array_equal(self.rows_of(read_row), self.state))
+        self.results.append({"leg": name, "round_trips": rounds, "ok": ok})
+        return ok
+
+    def summary(self):
+        return {"verified": all(r["ok"] for r in self.results) and bool(self.results),
+                "rows": [f"poly {p} limb {l}" for p, l in zip(self.polys, self.limbs)],
+                "checks": self.results,
+                "oracle": "UintNttTable restatement (oracle/primus_oracle.c), rows regenerated from the seed"}
+
+
+def device_row(nat, buf, stream):
+    def read(row):
+        out = np.empty(N, dtype=np.uint64)
+        nat.call("pg_memcpy_d2h", out.ctypes.data, buf.ptr + row * N * 8, N * 8, stream.h)
+        nat.call("pg_stream_synchronize", stream.h)
+        return out
+    return read
+
+
 def run_reference(args):
     # a CPU arm: under torchrun rank 0 alone times it and prints; the other ranks
     # exit without work (no process group, so nothing waits on them)
@@ -295,6 +351,10 @@ def run_gpu(args):
     ms_max = dist_max(dist, ms, local)
     per_step = ms_max / args.steps
     value = NTT_PER_STEP * world / (per_step / 1e3)
+    # every fused launch so far (warm-up and timed) is one round trip of the batch
+    rounds = args.warmup + args.steps
+    check = RowCheck(moduli, SEED + rank, cpu_threads())
+    check.check("timed fused launches", rounds, device_row(nat, data, stream))
 
     # ---- plain one-call-per-op GPU form (fwd, mul, inv as separate launches), same data
     for _ in range(2):
@@ -310,6 +370,8 @@ def run_gpu(args):
     e1.record(stream)
     stream.synchronize()
     plain_ms = e0.elapsed_ms(e1) / plain_steps
+    rounds += 2 + plain_steps
+    check.check("plain three-launch form", rounds, device_row(nat, data, stream))
 
     # ---- end to end through the public C ABI with pinned host buffers
     import ctypes as C
@@ -335,6 +397,8 @@ def run_gpu(args):
     e1.record(stream)
     stream.synchronize()
     e2e_ms = dist_max(dist, e0.elapsed_ms(e1) / e2e_steps, local)
+    check.check("end to end through the host-slice call", rounds + 2 + e2e_steps,
+                lambda row: host[row * N:(row + 1) * N].copy())
     nat.call("pg_host_free", hp.value)
     e2e_value = NTT_PER_STEP * world / (e2e_ms / 1e3)
 
@@ -354,6 +418,8 @@ def run_gpu(args):
         e1.record(stream)
         stream.synchronize()
         int_ms = e0.elapsed_ms(e1) / int_steps
+        rounds += 3 + int_steps
+        check.check("integer schedules only", rounds, device_row(nat, data, stream))
         tab.set_fp64(True)
         int_gbfly = NTT_PER_STEP * L * (N // 2) * LOG_N / (int_ms / 1e3) / 1e9
         integer_only = {"value": NTT_PER_STEP / (int_ms / 1e3), "unit": UNIT, "ms_per_step": int_ms,
@@ -413,6 +479,8 @@ def run_gpu(args):
                                      / cal["fp64_butterflies_gps" if tab.fp64 else "int_butterflies_gps"],
                              "source": "pg_calibrate: register-only forward butterflies of the same schedule"},
                          "builtin_copy_gbs": cal["hbm_copy_gbs"]},
+            "verified": check.summary()["verified"],
+            "verification": check.summary(),
             "integer_only": integer_only,
             "plain_gpu": {"value": NTT_PER_STEP / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                           "form": "pg_ntt_forward + pg_dcrt_mul + pg_ntt_inverse (3 launches)"},
