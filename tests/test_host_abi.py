@@ -37,6 +37,19 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(nat.lib(), s)
 
 
+def test_rust_bindings_declare_every_symbol():
+    """rust/primus_gpu/src/ffi.rs (the drop-in crate's bindings) declares exactly
+    the entry points of the header, with the same parameter counts."""
+    text = open(os.path.join(ROOT, "include", "primus_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    want = {m.group(1): (0 if m.group(2).strip() in ("", "void") else m.group(2).count(",") + 1)
+            for m in re.finditer(r"\b(pg_\w+)\s*\(([^)]*)\)\s*;", text)}
+    rs = open(os.path.join(ROOT, "rust", "primus_gpu", "src", "ffi.rs")).read()
+    got = {m.group(1): (0 if not m.group(2).strip() else m.group(2).count(",") + 1)
+           for m in re.finditer(r"pub fn (pg_\w+)\(([^)]*)\)", rs)}
+    assert got == want
+
+
 def test_status_strings():
     assert nat.lib().pg_status_string(0) == b"ok"
     assert nat.lib().pg_status_string(2) == b"no primitive root"
