@@ -315,7 +315,11 @@ def run_gpu(args):
     stream.synchronize()
     # kernel shape per (N, L): the autotuner times every shape of N = 2^16 on this
     # table before the warm-up and keeps the fastest in the table
-    tuning = tab.autotune(POLYS)
+    if args.no_tune:  # profiler captures: the default shapes, no tuning launches
+        tuning = {k: {"variant": 0, "name": "default", "us": 0.0, "default_us": 0.0}
+                  for k in ("forward", "inverse", "round_trip")}
+    else:
+        tuning = tab.autotune(POLYS)
     rt_shape = tuning["round_trip"]
     # built-in ceilings (streaming copy, register-only butterfly rates), measured before the warm-up
     cal = P.calibrate()
@@ -407,7 +411,7 @@ def run_gpu(args):
     integer_only = None
     if tab.fp64:
         tab.set_fp64(False)
-        int_tuning = tab.autotune(POLYS)
+        int_tuning = tab.autotune(POLYS) if not args.no_tune else {"round_trip": {"name": "default"}}
         for _ in range(3):
             step()
         stream.synchronize()
@@ -560,9 +564,19 @@ def bench_uneven(P, stream, jobs_n=512):
     singles = [batch.prepare([j]) for j in jobs]
     ms_graph = _time_stream(P, stream, lambda: batch.run(prepared, use_graph=True, stream=stream), 10)
     ms_plain = _time_stream(P, stream, lambda: [batch.run(j, use_graph=False, stream=stream) for j in singles], 3)
+    # tails: each degree class alone (its own launches, its own tail) against the
+    # whole set in one graph; and the butterfly rate against the fused
+    # round-trip kernel's (3 transforms of L rows per job: fwd a, fwd b, inv a)
+    per_class = {}
+    for ln in log_ns:
+        cls = batch.prepare([j for j in jobs if j[2] == ln])
+        per_class[f"N=2^{ln}"] = _time_stream(P, stream, lambda: batch.run(cls, use_graph=False, stream=stream), 5)
+    bfly = sum(3 * L * (1 << (ln - 1)) * ln for ln, L in shape)
     return {"workload": "512 products, N uniform in 2^10..2^16, L uniform in 1..32, one graph launch",
             "jobs": jobs_n, "ms_per_batch": ms_graph, "jobs_per_s": jobs_n / (ms_graph / 1e3),
             "algorithmic_gb": total_bytes / 1e9, "achieved_gbs": total_bytes / (ms_graph / 1e3) / 1e9,
+            "g_butterflies_per_s": bfly / (ms_graph / 1e3) / 1e9,
+            "per_class_alone_ms": per_class, "sum_of_classes_alone_ms": sum(per_class.values()),
             "plain_per_job_ms": ms_plain, "plain_jobs_per_s": jobs_n / (ms_plain / 1e3)}
 
 
@@ -917,6 +931,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default kernel shapes (no autotuner launches), for profiler captures")
     ap.add_argument("--polys", type=int, default=POLYS,
                     help="polys per step (default 128 = the workload; smaller only for profiler captures)")
     ap.add_argument("--workload", default=None,

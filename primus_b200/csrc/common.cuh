@@ -100,6 +100,18 @@ PG_DEV uint64_t shoup_mul(uint64_t w, uint64_t wq, uint64_t b, uint64_t q) {
 
 PG_DEV uint64_t reduce_once(uint64_t v, uint64_t m) { return v >= m ? v - m : v; }
 
+// Loads through explicitly global addresses.  A generic pointer may point into
+// shared memory, so a generic load that follows a store to shared memory in
+// program order cannot be issued before that store: a loop that stages global
+// values through shared memory would wait one full memory latency per element.
+// ld_stream (ld.global.cg, cached in L2 only) reads data the kernel streams
+// once; ld_table (ld.global.nc, the read-only path) reads tables no kernel
+// writes while it runs.
+PG_DEV uint64_t ld_stream(const uint64_t* p) { return __ldcg((const unsigned long long*)p); }
+PG_DEV uint64_t ld_table(const uint64_t* p) { return __ldg((const unsigned long long*)p); }
+// ld.global.ca: cached in L1 too, for per-thread runs of consecutive words
+PG_DEV uint64_t ld_cached(const uint64_t* p) { return __ldca((const unsigned long long*)p); }
+
 // UintModulus::reduce_add (primus_modulus/src/unsigned_integer/ops.rs:34-41)
 PG_DEV uint64_t add_mod(uint64_t a, uint64_t b, uint64_t m) {
     uint64_t s = a + b;

@@ -71,8 +71,12 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
     for (int i = 0; i < KP; ++i) {
         // this thread's coefficients tid + jj*T; it alone reads their digits back
         const uint64_t* src = a.in + (b * KP + i) * N;
+        // every global load is issued before the digits' shared-memory stores
+        uint64_t v[E];
 #pragma unroll
-        for (int jj = 0; jj < E; ++jj) decompose_word<DT, N>(src[tid + jj * T], a.gw, dg + tid + jj * T);
+        for (int jj = 0; jj < E; ++jj) v[jj] = ld_stream(src + tid + jj * T);
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) decompose_word<DT, N>(v[jj], a.gw, dg + tid + jj * T);
         for (uint32_t j = 0; j < d; ++j) {
             uint64_t x[E];
 #pragma unroll

@@ -481,6 +481,24 @@ PG_DEV void store_smem(const uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t b
     for (int jj = 0; jj < (1 << LOG_E); ++jj) p[padi(jj << G)] = x[jj];
 }
 
+// Barrier between two rounds whose E-element groups sit at bit G1 and G2 of
+// the element index (group_base inserts the group's LOG_E bits at G into the
+// thread index).  A warp's threads fix thread-index bits 5 .. LOG_T-1; each of
+// them lands at the same element bit in both rounds unless it lies in
+// [min(G1, G2), max(G1, G2)).  When none does, every warp stores and then
+// loads the same set of elements (and last read those locations itself), so a
+// warp barrier orders the exchange; otherwise the whole CTA synchronises.
+// With 32 or fewer threads per row every exchange stays inside one warp.
+template <int LOG_T, int G1, int G2>
+PG_DEV void exchange_sync() {
+    constexpr int lo = G1 < G2 ? G1 : G2, hi = G1 < G2 ? G2 : G1;
+    constexpr bool warp_local = LOG_T <= 5 || hi <= 5 || lo >= LOG_T;
+    if constexpr (warp_local)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
 // Forward rounds over the low TOP bits of a block (the bits above TOP were
 // processed earlier): round R covers bits [P_LO, P_HI], its group spans
 // [P_LO, P_LO + LOG_E).
@@ -503,7 +521,7 @@ PG_DEV void fwd_rest(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uint
         using Cur = FwdRounds<TOP, LOG_E, R>;
         using Prev = FwdRounds<TOP, LOG_E, R - 1>;
         store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
-        __syncthreads();
+        exchange_sync<LOG_M - LOG_E, Prev::G, Cur::G>();
         const uint32_t base = group_base<LOG_E>(tid, Cur::G);
         load_smem<LOG_E, Cur::G>(x, sm, base);
         fwd_round<LOG_M, LOG_E, Cur::G, Cur::P_HI, Cur::P_LO, FAST>(x, base, tw_base, tw, q2, nq);
@@ -530,7 +548,7 @@ PG_DEV void inv_range(uint64_t (&x)[1 << LOG_E], uint64_t* sm, uint32_t tid, uin
         using Cur = InvRounds<TOP, LOG_E, R>;
         using Prev = InvRounds<TOP, LOG_E, R - 1>;
         store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
-        __syncthreads();
+        exchange_sync<LOG_M - LOG_E, Prev::G, Cur::G>();
         const uint32_t base = group_base<LOG_E>(tid, Cur::G);
         load_smem<LOG_E, Cur::G>(x, sm, base);
         inv_round<LOG_N, LOG_M, LOG_E, Cur::G, Cur::P_LO, Cur::P_HI, FASTI>(x, base, rank, itw, sptr, srptr, q, nq,
@@ -663,12 +681,19 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
         const uint64_t iA = FP ? as_u(fm.q) : q, iB = FP ? as_u(fm.qinv) : nq;
         using I0 = InvRounds<LOG_N, LOG_E, 0>;
         if constexpr (MODE == MODE_INV) {
-            // stage the bit-reversed row through smem (coalesced), then round 0
+            // stage the bit-reversed row through smem (coalesced), then round 0;
+            // every global load is issued before the first shared-memory store
+#pragma unroll
+            for (int k = 0; k < E; ++k) x[k] = active ? ld_stream(g + tid + k * T) : 0;
+            // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+            if (mulp && active) {
+                const Barrett bar = a.bar[limb];
+#pragma unroll
+                for (int k = 0; k < E; ++k) x[k] = barrett_mul(x[k], ld_stream(mulp + tid + k * T), bar);
+            }
 #pragma unroll
             for (int k = 0; k < E; ++k) {
-                uint64_t v = active ? g[tid + k * T] : 0;
-                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
-                if (mulp && active) v = barrett_mul(v, mulp[tid + k * T], a.bar[limb]);
+                uint64_t v = x[k];
                 if constexpr (FP) v = as_u(freduce(u52_to_f(v), fm.q, fm.qinv));  // inputs < 2q < 2^52
                 sm[padi(tid + k * T)] = v;
             }
@@ -722,9 +747,13 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
 // other's barrier and exchange phases.
 __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
 
+// One row of the cluster kernel: row u of the launch (see ntt_cluster_kernel).
+// `first` is false when this cluster already processed an earlier row in the
+// same launch: the forward's opening cluster arrive is then a release, so
+// that every CTA's shared-memory reads of the previous row are ordered before
+// any other CTA's remote stores of this row.
 template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
-__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
-    ntt_cluster_kernel(NttArgs a) {
+PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const bool first) {
     constexpr bool FP = S == kSchedFp64;
     constexpr int KF = FP ? 2 : (S >= 1 ? 1 : 0), KI = FP ? 2 : (S >= 2 ? 1 : 0);  // round kinds
     constexpr bool FAST = KF == 1, FASTI = KI == 1;
@@ -735,13 +764,10 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
     constexpr int TOP = LOG_M - LOG_K;    // block bits handled by the local rounds
     constexpr int GX = LOG_N - LOG_E;     // cross group stride bit (N/E)
     static_assert(LOG_K >= 0 && TOP >= LOG_E, "shape");
-    extern __shared__ uint64_t smem_cl[];
-    uint64_t* sm = smem_cl;
     const uint32_t tid = threadIdx.x;
     const uint32_t rank = blockIdx.x & ((1 << LOG_C) - 1);
-    // grid is exactly rows * C; clusters run limb-major so that concurrently
-    // running clusters share one prime's twiddles in L2
-    const uint64_t u = blockIdx.x >> LOG_C;
+    // rows run limb-major so that concurrently running clusters share one
+    // prime's twiddles in L2
     const uint64_t polys = a.desc ? 1 : a.rows / a.L;  // descriptor rows need no [P][L] shape
     uint32_t limb = (uint32_t)(u / polys);
     const uint64_t row = (u % polys) * a.L + limb;
@@ -764,8 +790,11 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
         const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         // matched by the wait before the first remote store; relaxed is enough
-        // because this CTA has not touched shared memory yet
-        cluster_arrive_relaxed();
+        // on a cluster's first row, when this CTA has not touched shared memory yet
+        if (first)
+            cluster_arrive_relaxed();
+        else
+            cluster_arrive_release();
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) {
             x[jj] = g[gt + (jj << GX)];
@@ -828,12 +857,19 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
         using ILast = InvRounds<TOP, LOG_E, I0::COUNT - 1>;
         static_assert(I0::COUNT >= 2, "cluster path needs two local rounds");
         if constexpr (MODE == MODE_INV) {
-            uint64_t* gb = g + rank * M;
+            // every global load is issued before the first shared-memory store
+            const uint64_t* gb = g + rank * M;
+#pragma unroll
+            for (int k = 0; k < E; ++k) x[k] = ld_stream(gb + tid + k * T);
+            // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
+            if (mulp) {
+                const Barrett bar = a.bar[limb];
+#pragma unroll
+                for (int k = 0; k < E; ++k) x[k] = barrett_mul(x[k], ld_stream(mulp + rank * M + tid + k * T), bar);
+            }
 #pragma unroll
             for (int k = 0; k < E; ++k) {
-                uint64_t v = gb[tid + k * T];
-                // descriptor rows may carry an NTT-domain multiplicand (canonical inputs)
-                if (mulp) v = barrett_mul(v, mulp[rank * M + tid + k * T], a.bar[limb]);
+                uint64_t v = x[k];
                 if constexpr (FP) v = as_u(freduce(u52_to_f(v), fm.q, fm.qinv));  // inputs < 2q < 2^52
                 sm[padi(tid + k * T)] = v;
             }
@@ -850,7 +886,7 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
             // CTA overwrites a block that another CTA is still reading
             using Prev = InvRounds<TOP, LOG_E, I0::COUNT - 2>;
             store_smem<LOG_E, Prev::G>(x, sm, group_base<LOG_E>(tid, Prev::G));
-            __syncthreads();
+            exchange_sync<LOG_T, Prev::G, ILast::G>();
             const uint32_t base = group_base<LOG_E>(tid, ILast::G);
             load_smem<LOG_E, ILast::G>(x, sm, base);
             // release: these shared-memory reads must be performed before any
@@ -882,6 +918,41 @@ __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << 
     }
 }
 
+// The cluster kernel: a grid of rows * C CTAs runs one row per cluster; a
+// persistent grid (as many clusters as are resident at once) walks the rows
+// with a stride of its cluster count, which removes the gaps between cluster
+// launches and keeps each cluster on consecutive rows of one limb.
+// MINB: CTAs per SM the register budget is sized for (0: cluster_min_blocks).
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, int MINB = 0>
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), MINB ? MINB : cluster_min_blocks(1 << (LOG_M - LOG_E)))
+    ntt_cluster_kernel(NttArgs a) {
+    extern __shared__ uint64_t smem_cl[];
+    constexpr int LOG_C = LOG_N - LOG_M;
+    const uint64_t clusters = gridDim.x >> LOG_C;
+    for (uint64_t u = blockIdx.x >> LOG_C; u < a.rows; u += clusters)
+        cluster_row<LOG_N, LOG_M, LOG_E, MODE, S>(a, smem_cl, u, u < clusters);
+}
+
+// Both pipes in one launch (every q < 2^50): rows u with bit (u mod 8) of
+// INT_MASK set run the integer schedules (Shoup products on the integer
+// multiply pipe), the others the FP64 schedule.  The two kinds of CTAs share
+// SMs, so the FP64 pipe and the integer multiply pipe work at the same time.
+// Every row's values are the canonical residues either way.
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int INT_MASK>
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
+    ntt_cluster_dual_kernel(NttArgs a) {
+    extern __shared__ uint64_t smem_cl[];
+    constexpr int LOG_C = LOG_N - LOG_M;
+    constexpr int SI = MODE == MODE_FWD ? kSchedFastFwd : kSchedFastBoth;
+    const uint64_t clusters = gridDim.x >> LOG_C;
+    for (uint64_t u = blockIdx.x >> LOG_C; u < a.rows; u += clusters) {
+        if ((INT_MASK >> (u & 7)) & 1)
+            cluster_row<LOG_N, LOG_M, LOG_E, MODE, SI>(a, smem_cl, u, u < clusters);
+        else
+            cluster_row<LOG_N, LOG_M, LOG_E, MODE, kSchedFp64>(a, smem_cl, u, u < clusters);
+    }
+}
+
 }  // namespace pg
 
 namespace pg {
@@ -904,11 +975,19 @@ static int launch_block(const NttArgs& a, cudaStream_t st) {
     return PG_OK;
 }
 
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
-static int launch_cluster(const NttArgs& a, cudaStream_t st) {
+// persistent: launch only as many clusters as the device holds at once (each
+// then walks several rows); otherwise one cluster per row.  DUAL >= 0 launches
+// the two-pipe kernel with INT_MASK = DUAL instead (S unused).
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, int MINB = 0, int DUAL = -1>
+static int launch_cluster(const NttArgs& a, cudaStream_t st, bool persistent = false) {
     constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
     constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
-    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S>;
+    auto kern = [] {
+        if constexpr (DUAL >= 0)
+            return ntt_cluster_dual_kernel<LOG_N, LOG_M, LOG_E, MODE, (DUAL >= 0 ? DUAL : 0)>;
+        else
+            return ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S, MINB>;
+    }();
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
     if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
@@ -927,6 +1006,17 @@ static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     if constexpr (C > 8) {
         static const cudaError_t np = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (np != cudaSuccess) return cuda_status(np, "ntt_cluster_kernel: non-portable cluster size");
+    }
+    if (persistent) {
+        // resident clusters of this shape (block size, shared memory and cluster
+        // size; the grid does not enter), asked once; 0 if the query fails,
+        // which leaves the one-cluster-per-row grid
+        static const int resident = [&] {
+            int n = 0;
+            return cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess ? n : 0;
+        }();
+        cudaGetLastError();  // a failed query leaves no error behind for the launch check
+        if (resident > 0 && (uint64_t)resident < a.rows) cfg.gridDim = dim3((unsigned)(resident * C));
     }
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
     count_launch();

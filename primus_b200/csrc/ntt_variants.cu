@@ -43,51 +43,36 @@ constexpr VariantInfo kVariants[] = {
     {15, 3, "fp64 cluster of 8 x 4096", true},    {15, 4, "fp64 cluster of 4 x 8192", true},
     {16, 1, "cluster of 8 x 8192", false},        {16, 2, "fp64 cluster of 16 x 4096", true},
     {16, 3, "fp64 cluster of 8 x 8192", true},
+    // persistent grids: as many clusters as are resident, each walking rows
+    {13, 6, "fp64 cluster of 2 x 4096, persistent", true},
+    {14, 6, "fp64 cluster of 4 x 4096, persistent", true},
+    {15, 5, "fp64 cluster of 8 x 4096, persistent", true},
+    {16, 4, "fp64 cluster of 16 x 4096, persistent", true},
+    {16, 5, "fp64 cluster of 8 x 8192, persistent", true},
+    {16, 6, "cluster of 16 x 4096, persistent", false},
+    // register budgets for 3 and 5 CTAs per SM (85 and 51 registers per thread)
+    {16, 7, "fp64 cluster of 16 x 4096, 3 CTAs per SM", true},
+    {16, 8, "fp64 cluster of 16 x 4096, 5 CTAs per SM", true},
+    // both pipes: 1/4, 3/8 and 1/2 of the rows on the integer schedule
+    {16, 9, "dual pipe cluster of 16 x 4096, 1/4 integer rows", true},
+    {16, 10, "dual pipe cluster of 16 x 4096, 3/8 integer rows", true},
+    {16, 11, "dual pipe cluster of 16 x 4096, 1/2 integer rows", true},
+    {15, 6, "dual pipe cluster of 8 x 4096, 3/8 integer rows", true},
+    // 32 elements per thread: 16-CTA clusters of 128 threads at 4, 5 and 6 CTAs
+    // per SM (128, 102 and 85 registers), and 8-CTA clusters of 8192 at 3 per SM
+    {16, 12, "fp64 cluster of 16 x 4096, E=32, 4 CTAs per SM", true},
+    {16, 13, "fp64 cluster of 16 x 4096, E=32, 5 CTAs per SM", true},
+    {16, 14, "fp64 cluster of 16 x 4096, E=32, 6 CTAs per SM", true},
+    {16, 15, "fp64 cluster of 8 x 8192, E=32, 3 CTAs per SM", true},
 };
 
-template <int MODE>
-int run_variant(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
-    // the integer variants run the fast schedules: the forward every q < 2^58,
-    // the inverse and the round trip every q < 2^50 (canonical outputs); the
-    // FP64 variants every q < 2^50
-    constexpr int F = MODE == MODE_FWD ? kSchedFastFwd : kSchedFastBoth;
-    constexpr int D = kSchedFp64;
-    switch (log_n * 8 + (uint32_t)v) {
-        case 10 * 8 + 1: return launch_block<10, 3, 2, MODE, F>(a, st);
-        case 10 * 8 + 2: return launch_block<10, 2, 1, MODE, F>(a, st);
-        case 11 * 8 + 1: return launch_block<11, 4, 1, MODE, F>(a, st);
-        case 11 * 8 + 2: return launch_block<11, 4, 2, MODE, F>(a, st);
-        case 12 * 8 + 1: return launch_block<12, 3, 1, MODE, F>(a, st);
-        case 12 * 8 + 2: return launch_block<12, 4, 2, MODE, F>(a, st);
-        case 12 * 8 + 3: return launch_cluster<12, 11, 4, MODE, F>(a, st);
-        case 13 * 8 + 1: return launch_block<13, 3, 1, MODE, F>(a, st);
-        case 13 * 8 + 2: return launch_block<13, 4, 1, MODE, F>(a, st);
-        case 13 * 8 + 3: return launch_cluster<13, 11, 4, MODE, F>(a, st);
-        case 14 * 8 + 1: return launch_cluster<14, 13, 4, MODE, F>(a, st);
-        case 14 * 8 + 2: return launch_block<14, 4, 1, MODE, F>(a, st);
-        case 14 * 8 + 3: return launch_cluster<14, 11, 4, MODE, F>(a, st);
-        case 15 * 8 + 1: return launch_cluster<15, 13, 4, MODE, F>(a, st);
-        case 15 * 8 + 2: return launch_cluster<15, 11, 4, MODE, F>(a, st);
-        case 16 * 8 + 1: return launch_cluster<16, 13, 4, MODE, F>(a, st);
-        case 10 * 8 + 3: return launch_block<10, 3, 1, MODE, D>(a, st);
-        case 10 * 8 + 4: return launch_block<10, 3, 2, MODE, D>(a, st);
-        case 11 * 8 + 3: return launch_block<11, 3, 1, MODE, D>(a, st);
-        case 11 * 8 + 4: return launch_block<11, 4, 1, MODE, D>(a, st);
-        case 12 * 8 + 4: return launch_block<12, 4, 1, MODE, D>(a, st);
-        case 12 * 8 + 5: return launch_cluster<12, 11, 4, MODE, D>(a, st);
-        case 13 * 8 + 4: return launch_cluster<13, 12, 4, MODE, D>(a, st);
-        case 13 * 8 + 5: return launch_cluster<13, 11, 4, MODE, D>(a, st);
-        case 14 * 8 + 4: return launch_cluster<14, 12, 4, MODE, D>(a, st);
-        case 14 * 8 + 5: return launch_cluster<14, 13, 4, MODE, D>(a, st);
-        case 15 * 8 + 3: return launch_cluster<15, 12, 4, MODE, D>(a, st);
-        case 15 * 8 + 4: return launch_cluster<15, 13, 4, MODE, D>(a, st);
-        case 16 * 8 + 2: return launch_cluster<16, 12, 4, MODE, D>(a, st);
-        case 16 * 8 + 3: return launch_cluster<16, 13, 4, MODE, D>(a, st);
-    }
-    return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
-}
-
 }  // namespace
+
+// the shape instantiations live in ntt_shapes_*.cu (one family per translation unit)
+int run_ntt_shape_lo(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
+int run_ntt_shape_mid(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
+int run_ntt_shape_hi_a(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
+int run_ntt_shape_hi_b(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
 
 int ntt_variant_count(uint32_t log_n) {
     int c = 1;
@@ -110,12 +95,10 @@ const char* ntt_variant_name(uint32_t log_n, int variant) {
 }
 
 int launch_ntt_variant(const NttArgs& a, uint32_t log_n, int mode, int variant, cudaStream_t st) {
-    switch (mode) {
-        case MODE_FWD: return run_variant<MODE_FWD>(a, log_n, variant, st);
-        case MODE_INV: return run_variant<MODE_INV>(a, log_n, variant, st);
-        case MODE_RT: return run_variant<MODE_RT>(a, log_n, variant, st);
-    }
-    return set_error(PG_ERR_INVALID_ARGUMENT, "bad NTT mode");
+    if (log_n <= 13) return run_ntt_shape_lo(a, log_n, mode, variant, st);
+    if (log_n <= 15) return run_ntt_shape_mid(a, log_n, mode, variant, st);
+    return variant <= 6 ? run_ntt_shape_hi_a(a, log_n, mode, variant, st)
+                        : run_ntt_shape_hi_b(a, log_n, mode, variant, st);
 }
 
 }  // namespace pg

@@ -339,16 +339,20 @@ __global__ void __launch_bounds__(128) gadget_kernel(GadgetArgs a) {
     const uint64_t half = (a.basis + 1) / 2;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < a.count; x += (size_t)gridDim.x * blockDim.x) {
         const uint64_t* src = a.vals + x * a.W;
-        for (uint32_t k = 0; k < a.W; ++k) v[k] = src[k];
+        // global loads (not generic ones, which would wait for each preceding
+        // shared-memory store), so the W limbs are requested back to back
+        for (uint32_t k = 0; k < a.W; ++k) v[k] = ld_cached(src + k);
         v[a.W] = 0;  // guard limb for the straddling mask read (its mask is 0 there)
         if (a.has_split) {
             int cmp = 0;
-            for (uint32_t k = a.W; k-- > 0;)
-                if (cmp == 0 && v[k] != a.split[k]) cmp = v[k] < a.split[k] ? -1 : 1;
+            for (uint32_t k = a.W; k-- > 0;) {
+                const uint64_t sk = ld_table(a.split + k);
+                if (cmp == 0 && v[k] != sk) cmp = v[k] < sk ? -1 : 1;
+            }
             if (cmp >= 0) {
                 uint64_t carry = 0;
                 for (uint32_t k = 0; k < a.W; ++k) {
-                    uint64_t s = v[k] + a.npq[k];
+                    uint64_t s = v[k] + ld_table(a.npq + k);
                     uint64_t c1 = s < v[k];
                     uint64_t s2 = s + carry;
                     uint64_t c2 = s2 < s;
@@ -359,7 +363,17 @@ __global__ void __launch_bounds__(128) gadget_kernel(GadgetArgs a) {
         }
         uint64_t carry = a.has_init ? ((v[a.init_index] & a.init_mask) != 0) : 0;
         for (uint32_t j = 0; j < a.d; ++j) {
-            const DigitMask m = a.masks[j];
+            DigitMask m;  // read-only path (the generic load would wait for the stores above)
+            {
+                const ulonglong2 m0 = __ldg(reinterpret_cast<const ulonglong2*>(a.masks + j));
+                const ulonglong2 m1 = __ldg(reinterpret_cast<const ulonglong2*>(a.masks + j) + 1);
+                m.index = (uint32_t)m0.x;
+                m.shr = (uint32_t)(m0.x >> 32);
+                m.shl = (uint32_t)m0.y;
+                m.pad = (uint32_t)(m0.y >> 32);
+                m.mask0 = m1.x;
+                m.mask1 = m1.y;
+            }
             uint64_t temp = (v[m.index] & m.mask0) >> m.shr;
             if (m.mask1 != 0) temp |= (v[m.index + 1] & m.mask1) << m.shl;
             temp += carry;
@@ -369,7 +383,7 @@ __global__ void __launch_bounds__(128) gadget_kernel(GadgetArgs a) {
             if constexpr (LIFT) {
                 uint64_t* o = a.out + ((p * a.d + j) * a.L) * a.n + c;
                 for (uint32_t l = 0; l < a.L; ++l)
-                    o[(size_t)l * a.n] = (a.basis == 2 || digit < half) ? digit : a.moduli[l] - a.basis + digit;
+                    o[(size_t)l * a.n] = (a.basis == 2 || digit < half) ? digit : ld_table(a.moduli + l) - a.basis + digit;
             } else {
                 a.out[(p * a.d + j) * a.n + c] = digit;
             }
