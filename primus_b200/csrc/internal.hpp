@@ -137,6 +137,12 @@ struct NttArgs {
     const ulonglong2* inv_n_fp;
     const ulonglong2* inv_last_fp;
     const RowDesc* desc;  // NULL: rows are [polys][L][N] at data
+    // forward launches only: when set, row pd * L + limb reads gadget digit row
+    // pd ([N] words at lift_src + pd * N) and lifts each digit mod q_limb on the
+    // fly (digit < lift_half stays, else q - lift_basis + digit), writing the
+    // transform to data; NULL: rows are read from data
+    const uint64_t* lift_src;
+    uint64_t lift_basis, lift_half;
     uint64_t rows;
     uint64_t max_modulus;
     uint32_t L;
@@ -184,6 +190,8 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
     a.inv_n_fp = t->d_inv_n_fp;
     a.inv_last_fp = t->d_inv_last_fp;
     a.desc = nullptr;
+    a.lift_src = nullptr;
+    a.lift_basis = a.lift_half = 0;
     a.rows = rows;
     a.max_modulus = 0;
     for (uint64_t m : t->moduli) a.max_modulus = m > a.max_modulus ? m : a.max_modulus;

@@ -12,8 +12,9 @@
 //   key-switching key = k_in GLevs over k_out+1 output polys (key_switch.rs:17-24)
 //
 // Batched pipeline (one launch per step for the whole batch): CRT compose of
-// every input poly -> signed gadget digits lifted into the RNS base -> forward
-// NTT of every digit row -> one multiply-accumulate kernel that forms every
+// every input poly -> signed gadget digits -> forward NTT of every digit row
+// lifted into each limb of the RNS base as the transform loads it -> one
+// multiply-accumulate kernel that forms every
 // output coefficient as sum_{i,j} key[i][j][c] * digit[i][j] with a 128-bit
 // accumulator.  Outputs are canonical NTT-domain residues, equal to the
 // reference's sequential per-digit MAC.
@@ -30,6 +31,7 @@ uint32_t rns_W(const pg_rns_base* b);
 const uint64_t* rns_moduli(const pg_rns_base* b);
 const pg_rns_base* gadget_base(const pg_gadget_basis* g);
 uint32_t gadget_d(const pg_gadget_basis* g);
+uint64_t gadget_basis_value(const pg_gadget_basis* g);
 bool gadget_word(const pg_gadget_basis* g, GadgetWord* out);
 int launch_compose(const pg_rns_base* b, const uint64_t* res, uint64_t* out, size_t count, size_t n, uint32_t ppg,
                    size_t group_stride, cudaStream_t st);
@@ -195,16 +197,17 @@ int check_compat(const pg_ntt_table* t, const pg_gadget_basis* g) {
     return PG_OK;
 }
 
-// workspace: BigUint values [P][N][W] + lifted digits [P][d][L][N] (+ extra).
+// workspace: BigUint values [P][N][W] + digits [P][d][N] + NTT-domain digit
+// rows [P][d][L][N] (+ extra).
 // Every product and sum is overflow-checked: a size that does not fit size_t
 // returns SIZE_MAX, which no workspace, pool or fixed array satisfies, so a
 // huge batch is refused on the host instead of wrapping to a small size.
 size_t ws_bytes(const pg_ntt_table* t, const pg_gadget_basis* g, size_t polys, size_t extra_words) {
     const pg_rns_base* b = gadget_base(g);
     size_t per = 0, words = 0, bytes = 0;
-    // words per poly: N * W (BigUint values) + d * L * N (lifted digit rows);
-    // (N <= 2^16, W <= 64 limbs, d <= 4096 digits, L <= 64 moduli: below 2^35)
-    const size_t per_poly = t->n * rns_W(b) + (size_t)gadget_d(g) * t->L * t->n;
+    // words per poly: N * W (BigUint values) + d * N (digits) + d * L * N (digit
+    // rows); (N <= 2^16, W <= 64 limbs, d <= 4096 digits, L <= 64 moduli: below 2^36)
+    const size_t per_poly = t->n * rns_W(b) + (size_t)gadget_d(g) * t->n + (size_t)gadget_d(g) * t->L * t->n;
     if (__builtin_mul_overflow(polys, per_poly, &per)) return SIZE_MAX;
     if (__builtin_add_overflow(per, extra_words, &words)) return SIZE_MAX;
     if (__builtin_mul_overflow(words, sizeof(uint64_t), &bytes)) return SIZE_MAX;
@@ -240,25 +243,35 @@ int get_workspace(Workspace& w, void* given, size_t given_bytes, size_t need, cu
     return PG_OK;
 }
 
-// compose (when the input is CRT residues) + lifted digits + forward NTT of
-// every digit row; returns the digit buffer inside the workspace
+// compose (when the input is CRT residues) + signed gadget digits + forward NTT
+// of every digit row lifted into every limb; returns the NTT-domain digit rows
+// [P][d][L][N] inside the workspace.  The digits are written once per
+// coefficient ([P][d][N]) and the forward NTT lifts them mod each q_l as it
+// loads them, so the L-fold lifted rows never pass through HBM before the
+// transform.
 int digits_pipeline(const pg_ntt_table* t, const pg_gadget_basis* g, const uint64_t* in, bool in_is_crt,
                     size_t polys, uint32_t ppg, size_t group_stride, uint64_t* ws, uint64_t** digits_out,
                     cudaStream_t st) {
     const pg_rns_base* b = gadget_base(g);
     const size_t n = t->n;
     const size_t count = polys * n;
+    const uint32_t d = gadget_d(g);
     uint64_t* big = ws;
-    uint64_t* dig = ws + count * rns_W(b);
+    uint64_t* small = ws + count * rns_W(b);
+    uint64_t* dig = small + count * d;
     const uint64_t* vals = in;
     if (in_is_crt) {
         int rc = launch_compose(b, in, big, count, n, ppg, group_stride, st);
         if (rc) return rc;
         vals = big;
     }
-    int rc = launch_gadget(g, vals, dig, count, n, true, st);
+    int rc = launch_gadget(g, vals, small, count, n, false, st);
     if (rc) return rc;
-    rc = launch_ntt(make_args(t, dig, polys * gadget_d(g) * (size_t)t->L, 0), t->log_n, MODE_FWD, st);
+    NttArgs a = make_args(t, dig, polys * d * (size_t)t->L, 0);
+    a.lift_src = small;
+    a.lift_basis = gadget_basis_value(g);
+    a.lift_half = a.lift_basis == 2 ? 2 : (a.lift_basis + 1) / 2;
+    rc = launch_ntt(a, t->log_n, MODE_FWD, st);
     if (rc) return rc;
     *digits_out = dig;
     return PG_OK;

@@ -41,6 +41,13 @@ namespace cg = cooperative_groups;
 namespace pg {
 
 PG_DEV int padi(int i) { return i + (i >> 4); }
+
+// a signed gadget digit (stored as digit < basis) lifted mod q:
+// RNSBase::wrapping_decompose_small_values_inplace (primus_rns/src/base.rs:201-231);
+// half = 2 for basis 2 (both digits stay), else (basis + 1) / 2
+PG_DEV uint64_t lift_digit(uint64_t v, uint64_t q, uint64_t basis, uint64_t half) {
+    return v < half ? v : v + (q - basis);
+}
 __host__ __device__ constexpr int padded(int m) { return m + (m >> 4); }
 
 template <int V>
@@ -626,10 +633,13 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
         const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         using R0 = FwdRounds<LOG_N, LOG_E, 0>;
-        // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T]
+        // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T] (or the
+        // lifted gadget digits of the row's digit row)
+        const uint64_t* src = a.lift_src ? a.lift_src + (row / a.L) * N : g;
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) {
-            x[jj] = active ? g[tid + jj * T] : 0;
+            x[jj] = active ? src[tid + jj * T] : 0;
+            if (a.lift_src) x[jj] = lift_digit(x[jj], q, a.lift_basis, a.lift_half);
             if constexpr (FP) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
         }
         fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, KF>(x, tid, 1, tw, mA, mB);
@@ -748,12 +758,8 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
 __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
 
 // One row of the cluster kernel: row u of the launch (see ntt_cluster_kernel).
-// `first` is false when this cluster already processed an earlier row in the
-// same launch: the forward's opening cluster arrive is then a release, so
-// that every CTA's shared-memory reads of the previous row are ordered before
-// any other CTA's remote stores of this row.
 template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
-PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const bool first) {
+PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u) {
     constexpr bool FP = S == kSchedFp64;
     constexpr int KF = FP ? 2 : (S >= 1 ? 1 : 0), KI = FP ? 2 : (S >= 2 ? 1 : 0);  // round kinds
     constexpr bool FAST = KF == 1, FASTI = KI == 1;
@@ -790,14 +796,13 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const 
         const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
         const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         // matched by the wait before the first remote store; relaxed is enough
-        // on a cluster's first row, when this CTA has not touched shared memory yet
-        if (first)
-            cluster_arrive_relaxed();
-        else
-            cluster_arrive_release();
+        // because this CTA has not touched shared memory yet
+        cluster_arrive_relaxed();
+        const uint64_t* src = a.lift_src ? a.lift_src + (row / a.L) * N : g;  // digits to lift, or the row
 #pragma unroll
         for (int jj = 0; jj < E; ++jj) {
-            x[jj] = g[gt + (jj << GX)];
+            x[jj] = src[gt + (jj << GX)];
+            if (a.lift_src) x[jj] = lift_digit(x[jj], q, a.lift_basis, a.lift_half);
             if constexpr (FP) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
         }
         fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, KF>(x, gt, 1, tw, mA, mB);
@@ -918,39 +923,12 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const 
     }
 }
 
-// The cluster kernel: a grid of rows * C CTAs runs one row per cluster; a
-// persistent grid (as many clusters as are resident at once) walks the rows
-// with a stride of its cluster count, which removes the gaps between cluster
-// launches and keeps each cluster on consecutive rows of one limb.
-// MINB: CTAs per SM the register budget is sized for (0: cluster_min_blocks).
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, int MINB = 0>
-__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), MINB ? MINB : cluster_min_blocks(1 << (LOG_M - LOG_E)))
+// The cluster kernel: a grid of rows * C CTAs, one row per cluster of C CTAs.
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
+__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
     ntt_cluster_kernel(NttArgs a) {
     extern __shared__ uint64_t smem_cl[];
-    constexpr int LOG_C = LOG_N - LOG_M;
-    const uint64_t clusters = gridDim.x >> LOG_C;
-    for (uint64_t u = blockIdx.x >> LOG_C; u < a.rows; u += clusters)
-        cluster_row<LOG_N, LOG_M, LOG_E, MODE, S>(a, smem_cl, u, u < clusters);
-}
-
-// Both pipes in one launch (every q < 2^50): rows u with bit (u mod 8) of
-// INT_MASK set run the integer schedules (Shoup products on the integer
-// multiply pipe), the others the FP64 schedule.  The two kinds of CTAs share
-// SMs, so the FP64 pipe and the integer multiply pipe work at the same time.
-// Every row's values are the canonical residues either way.
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int INT_MASK>
-__global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
-    ntt_cluster_dual_kernel(NttArgs a) {
-    extern __shared__ uint64_t smem_cl[];
-    constexpr int LOG_C = LOG_N - LOG_M;
-    constexpr int SI = MODE == MODE_FWD ? kSchedFastFwd : kSchedFastBoth;
-    const uint64_t clusters = gridDim.x >> LOG_C;
-    for (uint64_t u = blockIdx.x >> LOG_C; u < a.rows; u += clusters) {
-        if ((INT_MASK >> (u & 7)) & 1)
-            cluster_row<LOG_N, LOG_M, LOG_E, MODE, SI>(a, smem_cl, u, u < clusters);
-        else
-            cluster_row<LOG_N, LOG_M, LOG_E, MODE, kSchedFp64>(a, smem_cl, u, u < clusters);
-    }
+    cluster_row<LOG_N, LOG_M, LOG_E, MODE, S>(a, smem_cl, blockIdx.x >> (LOG_N - LOG_M));
 }
 
 }  // namespace pg
@@ -975,19 +953,11 @@ static int launch_block(const NttArgs& a, cudaStream_t st) {
     return PG_OK;
 }
 
-// persistent: launch only as many clusters as the device holds at once (each
-// then walks several rows); otherwise one cluster per row.  DUAL >= 0 launches
-// the two-pipe kernel with INT_MASK = DUAL instead (S unused).
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, int MINB = 0, int DUAL = -1>
-static int launch_cluster(const NttArgs& a, cudaStream_t st, bool persistent = false) {
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
+static int launch_cluster(const NttArgs& a, cudaStream_t st) {
     constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
     constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
-    auto kern = [] {
-        if constexpr (DUAL >= 0)
-            return ntt_cluster_dual_kernel<LOG_N, LOG_M, LOG_E, MODE, (DUAL >= 0 ? DUAL : 0)>;
-        else
-            return ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S, MINB>;
-    }();
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
     if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
@@ -1006,17 +976,6 @@ static int launch_cluster(const NttArgs& a, cudaStream_t st, bool persistent = f
     if constexpr (C > 8) {
         static const cudaError_t np = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (np != cudaSuccess) return cuda_status(np, "ntt_cluster_kernel: non-portable cluster size");
-    }
-    if (persistent) {
-        // resident clusters of this shape (block size, shared memory and cluster
-        // size; the grid does not enter), asked once; 0 if the query fails,
-        // which leaves the one-cluster-per-row grid
-        static const int resident = [&] {
-            int n = 0;
-            return cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess ? n : 0;
-        }();
-        cudaGetLastError();  // a failed query leaves no error behind for the launch check
-        if (resident > 0 && (uint64_t)resident < a.rows) cfg.gridDim = dim3((unsigned)(resident * C));
     }
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
     count_launch();

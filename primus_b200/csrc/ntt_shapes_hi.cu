@@ -1,7 +1,6 @@
-// Kernel shapes the autotuner times for ring degree 2^16 (cluster shapes and
-// persistent grids): the instantiations behind launch_ntt_variant
-// (ntt_variants.cu), kept in a translation unit of their own so that the shape
-// families compile in parallel.
+// Kernel shapes the autotuner times for ring degree 2^16: the instantiations
+// behind launch_ntt_variant (ntt_variants.cu), kept in a translation unit of
+// their own so that the shape families compile in parallel.
 #include "ntt_kernels.cuh"
 
 namespace pg {
@@ -20,16 +19,13 @@ int run(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
         case 16 * 16 + 1: return launch_cluster<16, 13, 4, MODE, F>(a, st);
         case 16 * 16 + 2: return launch_cluster<16, 12, 4, MODE, D>(a, st);
         case 16 * 16 + 3: return launch_cluster<16, 13, 4, MODE, D>(a, st);
-        case 16 * 16 + 4: return launch_cluster<16, 12, 4, MODE, D>(a, st, true);
-        case 16 * 16 + 5: return launch_cluster<16, 13, 4, MODE, D>(a, st, true);
-        case 16 * 16 + 6: return launch_cluster<16, 12, 4, MODE, F>(a, st, true);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
 }
 
 }  // namespace
 
-int run_ntt_shape_hi_a(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st) {
+int run_ntt_shape_hi(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st) {
     switch (mode) {
         case MODE_FWD: return run<MODE_FWD>(a, log_n, v, st);
         case MODE_INV: return run<MODE_INV>(a, log_n, v, st);

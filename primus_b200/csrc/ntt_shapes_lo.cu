@@ -34,7 +34,6 @@ int run(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
         case 12 * 16 + 5: return launch_cluster<12, 11, 4, MODE, D>(a, st);
         case 13 * 16 + 4: return launch_cluster<13, 12, 4, MODE, D>(a, st);
         case 13 * 16 + 5: return launch_cluster<13, 11, 4, MODE, D>(a, st);
-        case 13 * 16 + 6: return launch_cluster<13, 12, 4, MODE, D>(a, st, true);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
 }

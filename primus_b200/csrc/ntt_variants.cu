@@ -43,27 +43,6 @@ constexpr VariantInfo kVariants[] = {
     {15, 3, "fp64 cluster of 8 x 4096", true},    {15, 4, "fp64 cluster of 4 x 8192", true},
     {16, 1, "cluster of 8 x 8192", false},        {16, 2, "fp64 cluster of 16 x 4096", true},
     {16, 3, "fp64 cluster of 8 x 8192", true},
-    // persistent grids: as many clusters as are resident, each walking rows
-    {13, 6, "fp64 cluster of 2 x 4096, persistent", true},
-    {14, 6, "fp64 cluster of 4 x 4096, persistent", true},
-    {15, 5, "fp64 cluster of 8 x 4096, persistent", true},
-    {16, 4, "fp64 cluster of 16 x 4096, persistent", true},
-    {16, 5, "fp64 cluster of 8 x 8192, persistent", true},
-    {16, 6, "cluster of 16 x 4096, persistent", false},
-    // register budgets for 3 and 5 CTAs per SM (85 and 51 registers per thread)
-    {16, 7, "fp64 cluster of 16 x 4096, 3 CTAs per SM", true},
-    {16, 8, "fp64 cluster of 16 x 4096, 5 CTAs per SM", true},
-    // both pipes: 1/4, 3/8 and 1/2 of the rows on the integer schedule
-    {16, 9, "dual pipe cluster of 16 x 4096, 1/4 integer rows", true},
-    {16, 10, "dual pipe cluster of 16 x 4096, 3/8 integer rows", true},
-    {16, 11, "dual pipe cluster of 16 x 4096, 1/2 integer rows", true},
-    {15, 6, "dual pipe cluster of 8 x 4096, 3/8 integer rows", true},
-    // 32 elements per thread: 16-CTA clusters of 128 threads at 4, 5 and 6 CTAs
-    // per SM (128, 102 and 85 registers), and 8-CTA clusters of 8192 at 3 per SM
-    {16, 12, "fp64 cluster of 16 x 4096, E=32, 4 CTAs per SM", true},
-    {16, 13, "fp64 cluster of 16 x 4096, E=32, 5 CTAs per SM", true},
-    {16, 14, "fp64 cluster of 16 x 4096, E=32, 6 CTAs per SM", true},
-    {16, 15, "fp64 cluster of 8 x 8192, E=32, 3 CTAs per SM", true},
 };
 
 }  // namespace
@@ -71,8 +50,7 @@ constexpr VariantInfo kVariants[] = {
 // the shape instantiations live in ntt_shapes_*.cu (one family per translation unit)
 int run_ntt_shape_lo(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
 int run_ntt_shape_mid(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
-int run_ntt_shape_hi_a(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
-int run_ntt_shape_hi_b(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
+int run_ntt_shape_hi(const NttArgs& a, uint32_t log_n, int mode, int v, cudaStream_t st);
 
 int ntt_variant_count(uint32_t log_n) {
     int c = 1;
@@ -97,8 +75,7 @@ const char* ntt_variant_name(uint32_t log_n, int variant) {
 int launch_ntt_variant(const NttArgs& a, uint32_t log_n, int mode, int variant, cudaStream_t st) {
     if (log_n <= 13) return run_ntt_shape_lo(a, log_n, mode, variant, st);
     if (log_n <= 15) return run_ntt_shape_mid(a, log_n, mode, variant, st);
-    return variant <= 6 ? run_ntt_shape_hi_a(a, log_n, mode, variant, st)
-                        : run_ntt_shape_hi_b(a, log_n, mode, variant, st);
+    return run_ntt_shape_hi(a, log_n, mode, variant, st);
 }
 
 }  // namespace pg

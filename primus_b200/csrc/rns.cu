@@ -125,6 +125,7 @@ uint32_t rns_L(const pg_rns_base* b) { return b->L; }
 uint32_t rns_W(const pg_rns_base* b) { return b->W; }
 const pg_rns_base* gadget_base(const pg_gadget_basis* g) { return g->base; }
 uint32_t gadget_d(const pg_gadget_basis* g) { return g->d; }
+uint64_t gadget_basis_value(const pg_gadget_basis* g) { return g->basis; }
 // the basis as single-word parameters; false when its values need more than one word
 bool gadget_word(const pg_gadget_basis* g, GadgetWord* out) {
     if (g->W != 1) return false;
