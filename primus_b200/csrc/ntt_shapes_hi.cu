@@ -19,6 +19,8 @@ int run(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
         case 16 * 16 + 1: return launch_cluster<16, 13, 4, MODE, F>(a, st);
         case 16 * 16 + 2: return launch_cluster<16, 12, 4, MODE, D>(a, st);
         case 16 * 16 + 3: return launch_cluster<16, 13, 4, MODE, D>(a, st);
+        case 16 * 16 + 4: return launch_cluster<16, 12, 4, MODE, D>(a, st, true);
+        case 16 * 16 + 5: return launch_cluster<16, 13, 4, MODE, D>(a, st, true);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
 }

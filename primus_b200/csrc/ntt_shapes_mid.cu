@@ -25,6 +25,8 @@ int run(const NttArgs& a, uint32_t log_n, int v, cudaStream_t st) {
         case 14 * 16 + 5: return launch_cluster<14, 13, 4, MODE, D>(a, st);
         case 15 * 16 + 3: return launch_cluster<15, 12, 4, MODE, D>(a, st);
         case 15 * 16 + 4: return launch_cluster<15, 13, 4, MODE, D>(a, st);
+        case 14 * 16 + 6: return launch_cluster<14, 12, 4, MODE, D>(a, st, true);
+        case 15 * 16 + 5: return launch_cluster<15, 12, 4, MODE, D>(a, st, true);
     }
     return set_error(PG_ERR_INVALID_ARGUMENT, "no such NTT kernel variant for this ring degree");
 }

@@ -43,6 +43,11 @@ constexpr VariantInfo kVariants[] = {
     {15, 3, "fp64 cluster of 8 x 4096", true},    {15, 4, "fp64 cluster of 4 x 8192", true},
     {16, 1, "cluster of 8 x 8192", false},        {16, 2, "fp64 cluster of 16 x 4096", true},
     {16, 3, "fp64 cluster of 8 x 8192", true},
+    // the same clusters with the spread placement policy (the default is load balancing)
+    {14, 6, "fp64 cluster of 4 x 4096, spread placement", true},
+    {15, 5, "fp64 cluster of 8 x 4096, spread placement", true},
+    {16, 4, "fp64 cluster of 16 x 4096, spread placement", true},
+    {16, 5, "fp64 cluster of 8 x 8192, spread placement", true},
 };
 
 }  // namespace
