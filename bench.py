@@ -687,6 +687,18 @@ def bench_widened(P, stream, batch=64):
                                                              stream=stream), 3)
     res["automorphism"] = {"us_per_ciphertext": ms * 1e3 / batch, "digits": g.d,
                            "rows_transformed_per_ciphertext": L + g.d * L}
+    # the reference-form key switch (CrtGlweKeySwitchingKey::key_swithching_inplace,
+    # BigUint gadget over all 16 limbs, 16 digits): coefficient-form input,
+    # NTT-domain output, k_in = k_out = 1
+    c_in = P.DeviceBuffer(batch * ct_words)
+    tab.fill_uniform(c_in, batch * (k + 1), seed=0x54, stream=stream)
+    kws = P.DeviceBuffer(P.key_switch_workspace_size(tab, g, k, k, batch) // 8 + 1)
+    ms = _time_stream(P, stream, lambda: P.key_switch(tab, g, k, k, key, c_in, out, batch, workspace=kws,
+                                                      stream=stream), 3)
+    res["key_switch_biguint_gadget"] = {"us_per_ciphertext": ms * 1e3 / batch, "digits": g.d,
+                                        "rows_transformed_per_ciphertext": L + g.d * L,
+                                        "path": "pg_key_switch: compose -> digits -> forward NTT lifting the "
+                                                "digits on load -> MAC"}
     return res
 
 
@@ -791,7 +803,7 @@ def bench_autotune(P):
     return out
 
 
-def bench_served(P, stream, count=2000, seed=0x5EED0005):
+def bench_served(P, stream, count=2000, seed=0x5EED0005, slots=4):
     """Mixed request stream: 50% RNS polymul (N = 2^12..2^16, L = 4..24), 30%
     external product (the N = 2048 shape above), 20% hybrid RNS key switch
     (N = 2^15, L = 16 plus K = 4 special primes, 4-limb digit groups, k = 1).  The plain form runs
@@ -880,7 +892,8 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
         return lat, time.perf_counter() - t0
 
     # ---- served
-    srv = P.Server(memory_budget_bytes=8 << 30, slots=4, max_batch=512, polymul_tables=list(pm_tables.values()))
+    srv = P.Server(memory_budget_bytes=2 * slots << 30, slots=slots, max_batch=512,
+                   polymul_tables=list(pm_tables.values()))
     xid = srv.register_key(2, xt, xg, 1, 1, xkey)
     kid = srv.register_hybrid_key(hks, 1, 1, kkey)
     reqs = []
@@ -923,7 +936,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005):
     return {"workload": "served mixed stream: 50% polymul N=2^12..2^16 L=4..24, 30% ext product (N=2048, k=1, "
                         "7-bit gadget), 20% hybrid key switch (N=2^15, L=16 + K=4 special primes, 4-limb digit "
                         "groups); Poisson arrivals",
-            "requests": count, "plain_capacity_rps": plain_rps, "per_kind": per_kind,
+            "requests": count, "slots": slots, "plain_capacity_rps": plain_rps, "per_kind": per_kind,
             "plain": plain_runs, "served": served_runs, "served_max_rps": best,
             "served_over_plain_capacity": best / plain_rps,
             "plain_p99_us_at_0_9x": plain_p99, "served_rps_at_plain_p99": at_p99,
