@@ -28,7 +28,10 @@
 // row -> the MAC kernel (Q and P limbs written apart) -> inverse NTT of the P
 // limbs -> pconv_kernel (P -> Q, scaled by P^-1, b added on the last output)
 // -> forward NTT of the converted rows -> finish_kernel.  Each step runs over
-// the whole batch in one launch.
+// the whole batch in one launch.  On the FP64 schedule at N = 2^13 .. 2^16 the
+// conversions run inside the transforms' loads and stores instead (the fused
+// form below): scale -> forward(ModUp on load) -> MAC -> inverse(P scaling on
+// store) -> forward(P -> Q on load, final combination on store).
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -307,6 +310,144 @@ __global__ void __launch_bounds__(256) finish_kernel(FinishArgs a) {
 
 
 
+// ---------------------------------------------------------------------------
+// Fused form (FP64 tables, N = 2^13 .. 2^16: the cluster transform).  The base
+// conversions move into the transforms' loads and stores, so the extended rows
+// and the converted rows never make a separate pass through HBM:
+//   scale_kernel: tv[p][l] = [a_p]_{q_l} * ((Q_g / q_l)^-1 mod q_l) for every Q limb
+//   forward NTT of the extended rows with ModUpIO: own-group limbs load a_p, the
+//     others load sum_m tv[p][lo + m] * ((Q_g / q_m) mod r) (ModUp on the integer
+//     pipe)
+//   MAC (unchanged)
+//   inverse NTT of the P limbs with PScaleIO: stores [acc_P]_{p_k} * ((P / p_k)^-1 mod p_k)
+//   forward NTT of the Q limbs with PConvIO: loads sum_k tvp[k] * ((P / p_k) P^-1 mod q_l)
+//     (+ b on the last output), stores NTT(..) - P^-1 acc_Q straight to the output
+// Same residues as the unfused sequence: every step is the same exact modular
+// arithmetic, and the transforms return canonical values for any input below 4q.
+// It runs for batches of at most kFusedMaxBatch key switches (see pg_key_switch_hybrid).
+// ---------------------------------------------------------------------------
+struct ScaleArgs {
+    const uint64_t* in;  // [B][k_in+1][L][N]
+    uint64_t* tv;        // [B * k_in][L][N]
+    const ulonglong2* ginv;
+    const uint64_t* moduli;
+    size_t polys, N;
+    uint32_t k_in, L, log_n;
+};
+
+// one thread per (mask, limb, coefficient); grid y = mask
+__global__ void __launch_bounds__(256) scale_kernel(ScaleArgs a) {
+    const uint32_t LN = a.L * (uint32_t)a.N;
+    for (size_t p = blockIdx.y; p < a.polys; p += gridDim.y) {
+        const size_t b = p / a.k_in, i = p % a.k_in;
+        const uint64_t* src = a.in + (b * (a.k_in + 1) + i) * LN;
+        uint64_t* dst = a.tv + p * LN;
+        for (uint32_t lx = blockIdx.x * blockDim.x + threadIdx.x; lx < LN; lx += gridDim.x * blockDim.x) {
+            const uint32_t l = lx >> a.log_n;
+            const ulonglong2 f = __ldg(a.ginv + l);
+            dst[lx] = shoup_mul(f.x, f.y, ld_stream(src + lx), ld_table(a.moduli + l));
+        }
+    }
+}
+
+// the extended rows ext[o][r] of o = (b k_in + i) dnum + g over the L + K limbs
+struct ModUpIO {
+    static constexpr bool kLoad = true, kStore = false;
+    const uint64_t* in;          // [B][k_in+1][L][N]
+    const uint64_t* tv;          // [B * k_in][L][N]
+    const ulonglong2* gmat;      // per group: [L+K-alpha_g][alpha_g] Shoup pairs
+    uint32_t k_in, L, K, alpha, dnum, log_n;
+
+    template <int E>
+    PG_DEV void load(uint64_t o, uint32_t r, uint64_t q, uint32_t i0, uint32_t stride, uint64_t (&x)[E]) const {
+        const uint32_t g = (uint32_t)(o % dnum);
+        const uint64_t p = o / dnum;
+        const uint32_t lo = g * alpha, hi = min(L, lo + alpha), ag = hi - lo;
+        if (r >= lo && r < hi) {  // the group's own limbs keep a_p's residues
+            const uint64_t* src = in + (((p / k_in) * (k_in + 1) + p % k_in) * L + r) * ((uint64_t)1 << log_n) + i0;
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = ld_stream(src + (size_t)jj * stride);
+            return;
+        }
+        // row j of the group's conversion matrix (every group before the last
+        // has alpha limbs, so the group's matrix starts at g (L + K - alpha) alpha)
+        const uint32_t j = r < lo ? r : r - ag;
+        const ulonglong2* mat = gmat + (size_t)g * (L + K - alpha) * alpha + (size_t)j * ag;
+        const uint64_t nq = 0 - q;
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = 0;
+        for (uint32_t m = 0; m < ag; ++m) {
+            const ulonglong2 w = __ldg(mat + m);
+            const uint64_t* t = tv + (p * L + lo + m) * ((uint64_t)1 << log_n) + i0;
+            // sums of at most 8 lazy products in [0, 2q): below 16q < 2^64
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] += shoup_lazy_nq(w.x, w.y, ld_cached(t + (size_t)jj * stride), nq);
+        }
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) {  // [0, 4q): a valid forward input
+            uint64_t v = x[jj];
+            v = v >= 8 * q ? v - 8 * q : v;
+            x[jj] = v >= 4 * q ? v - 4 * q : v;
+        }
+    }
+};
+
+// inverse transform of the P limbs of acc[p] (p = b KO + c, rows p * K + k):
+// stores [acc_P]_{p_k} * ((P / p_k)^-1 mod p_k), the scaled residues of the P -> Q conversion
+struct PScaleIO {
+    static constexpr bool kLoad = false, kStore = true;
+    uint64_t* accp;              // [B*KO][K][N]
+    const ulonglong2* pinv_k;    // [K]
+    uint32_t K, log_n;
+
+    PG_DEV void store(uint64_t p, uint32_t k, uint64_t q, uint32_t i, uint64_t v) const {
+        const ulonglong2 f = __ldg(pinv_k + k);
+        accp[((p * K + k) << log_n) + i] = shoup_mul(f.x, f.y, v, q);
+    }
+};
+
+// forward transform of the converted Q rows (p = b KO + c, rows p * L + l):
+// loads sum_k tvp[p][k] * ((P / p_k) P^-1 mod q_l) (+ b of ciphertext b on the
+// last output), stores NTT(..) - P^-1 acc_Q[p][l] to the output
+struct PConvIO {
+    static constexpr bool kLoad = true, kStore = true;
+    const uint64_t* tvp;         // [B*KO][K][N] (PScaleIO's stores)
+    const ulonglong2* pmat;      // [L][K]
+    const uint64_t* bsrc;        // b of ciphertext j at bsrc + j * bstride
+    size_t bstride;
+    const uint64_t* accq;        // [B*KO][L][N]
+    const ulonglong2* pinv;      // [L]
+    uint64_t* out;               // [B*KO][L][N]
+    uint32_t K, L, ko, log_n;
+
+    template <int E>
+    PG_DEV void load(uint64_t p, uint32_t l, uint64_t q, uint32_t i0, uint32_t stride, uint64_t (&x)[E]) const {
+        const uint64_t nq = 0 - q;
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) x[jj] = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            const ulonglong2 w = __ldg(pmat + (size_t)l * K + k);
+            const uint64_t* t = tvp + ((p * K + k) << log_n) + i0;
+            // sums of at most 8 lazy products in [0, 2q): below 16q
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] += shoup_lazy_nq(w.x, w.y, ld_cached(t + (size_t)jj * stride), nq);
+        }
+        const uint64_t* bp = (p % ko) == ko - 1 ? bsrc + (p / ko) * bstride + ((uint64_t)l << log_n) + i0 : nullptr;
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) {
+            uint64_t v = reduce_below_16q(x[jj], q);
+            if (bp) v += ld_stream(bp + (size_t)jj * stride);  // below 2q: a valid forward input
+            x[jj] = v;
+        }
+    }
+
+    PG_DEV void store(uint64_t p, uint32_t l, uint64_t q, uint32_t i, uint64_t v) const {
+        const size_t idx = ((p * L + l) << log_n) + i;
+        const ulonglong2 f = __ldg(pinv + l);
+        out[idx] = sub_mod(v, shoup_mul(f.x, f.y, ld_stream(accq + idx), q), q);
+    }
+};
+
 // a table view over limbs [first, first + count) of t (device arrays shared)
 void make_view(const pg_ntt_table* t, uint32_t first, uint32_t count, pg_ntt_table& v) {
     v.log_n = t->log_n;
@@ -359,10 +500,10 @@ uint64_t prod_except(const std::vector<uint64_t>& m, uint32_t lo, uint32_t hi, u
     return p;
 }
 
-// scratch words: ext | accQ | accP | conv
+// scratch words: ext | accQ | accP | conv | tv (the fused form's scaled masks)
 struct HybridWs {
-    size_t ext, accq, accp, conv;
-    size_t total() const { return ext + accq + accp + conv; }
+    size_t ext, accq, accp, conv, tv;
+    size_t total() const { return ext + accq + accp + conv + tv; }
 };
 
 HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t batch) {
@@ -372,7 +513,58 @@ HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t 
     w.accq = batch * KO * h->L * n;
     w.accp = batch * KO * h->K * n;
     w.conv = batch * KO * h->L * n;
+    w.tv = batch * k_in * h->L * n;
     return w;
+}
+
+// the fused transforms run the cluster kernel's default shape of each degree
+template <int MODE, class IO>
+int launch_fused_ntt(const NttArgs& a, uint32_t log_n, const IO& io, cudaStream_t st) {
+    switch (log_n) {
+        case 13: return launch_cluster<13, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
+        case 14: return launch_cluster<14, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
+        case 15: return launch_cluster<15, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
+        case 16: return launch_cluster<16, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
+    }
+    return set_error(PG_ERR_UNSUPPORTED, "fused key switch: ring degree outside 2^13 .. 2^16");
+}
+
+// largest batch that runs the fused form
+constexpr size_t kFusedMaxBatch = 8;
+
+// ModUp of every mask of every ciphertext, all groups, into ext (the separate kernel)
+int modup(const pg_hybrid_ks* h, uint32_t k_in, size_t batch, const uint64_t* d_in, uint64_t* ext, bool fp,
+          cudaStream_t st) {
+    const pg_ntt_table* t = h->t;
+    ModUpArgs ma{};
+    ma.in = d_in;
+    ma.ext = ext;
+    ma.ginv = h->d_ginv;
+    ma.gmat = h->d_gmat;
+    ma.gout = h->d_gout;
+    ma.gmat_off = h->d_offs;
+    ma.gout_off = h->d_offs + h->dnum;
+    ma.moduli = t->d_moduli;
+    ma.bar = t->d_barrett;
+    ma.polys = batch * k_in;
+    ma.N = t->n;
+    ma.k_in = k_in;
+    ma.L = h->L;
+    ma.K = h->K;
+    ma.alpha = h->alpha;
+    ma.dnum = h->dnum;
+    ma.log_n = t->log_n;
+    ma.gmat_fp = h->d_gmat_fp;
+    ma.fmod = h->d_fmod;
+    const dim3 mgrid = grid2((t->n + 1) / 2, ma.polys * h->dnum);
+    if (h->alpha <= 4)
+        fp ? modup_kernel<4, true><<<mgrid, 256, 0, st>>>(ma) : modup_kernel<4, false><<<mgrid, 256, 0, st>>>(ma);
+    else
+        fp ? modup_kernel<kMaxAlpha, true><<<mgrid, 256, 0, st>>>(ma)
+           : modup_kernel<kMaxAlpha, false><<<mgrid, 256, 0, st>>>(ma);
+    count_launch();
+    PG_LAUNCH_CHECK("modup_kernel launch");
+    return PG_OK;
 }
 
 struct OwnedWs {
@@ -523,43 +715,80 @@ int pg_key_switch_hybrid(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, c
     uint64_t* accq = ext + w.ext;
     uint64_t* accp = accq + w.accq;
     uint64_t* conv = accp + w.accp;
-    // ModUp of every mask of every ciphertext, all groups
-    ModUpArgs ma{};
-    ma.in = d_in;
-    ma.ext = ext;
-    ma.ginv = h->d_ginv;
-    ma.gmat = h->d_gmat;
-    ma.gout = h->d_gout;
-    ma.gmat_off = h->d_offs;
-    ma.gout_off = h->d_offs + h->dnum;
-    ma.moduli = t->d_moduli;
-    ma.bar = t->d_barrett;
-    ma.polys = batch * k_in;
-    ma.N = n;
-    ma.k_in = k_in;
-    ma.L = h->L;
-    ma.K = h->K;
-    ma.alpha = h->alpha;
-    ma.dnum = h->dnum;
-    ma.log_n = t->log_n;
+    uint64_t* tv = conv + w.conv;
     // the FP64 dot products when the table runs the FP64 schedule (every modulus below 2^50)
     const bool fp = h->d_fmod && t->fp64;
-    ma.gmat_fp = h->d_gmat_fp;
-    ma.fmod = h->d_fmod;
-    const dim3 mgrid = grid2((n + 1) / 2, ma.polys * h->dnum);
-    if (h->alpha <= 4)
-        fp ? modup_kernel<4, true><<<mgrid, 256, 0, st>>>(ma) : modup_kernel<4, false><<<mgrid, 256, 0, st>>>(ma);
-    else
-        fp ? modup_kernel<kMaxAlpha, true><<<mgrid, 256, 0, st>>>(ma)
-           : modup_kernel<kMaxAlpha, false><<<mgrid, 256, 0, st>>>(ma);
-    count_launch();
-    PG_LAUNCH_CHECK("modup_kernel launch");
-    int rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
-    if (rc) return rc;
+    // the fused form's last transform reads b from the input while it stores the
+    // outputs, so an output that overlaps the input takes the unfused sequence
+    const size_t in_words = batch * (k_in + 1) * L * n, out_words = batch * KO * L * n;
+    const bool overlap = d_in < d_out + out_words && d_out < d_in + in_words;
+    // The fused form pays off while launches and the serial chain of kernels
+    // dominate (N = 2^15, L = 16, K = 4: 150 -> 134 us for one key switch, 71 ->
+    // 70 us each in batches of 8); on a full GPU its integer dot products compete
+    // with the FP64 transforms, and the separate kernels are faster (batches of
+    // 32: 62.8 us separate, 65.0 us with only the P -> Q side fused, 70.3 us fused)
+    const bool fused = fp && !overlap && t->log_n >= 13 && t->log_n <= 16 && batch <= kFusedMaxBatch;
+    if (fused) {
+        ScaleArgs sa{};
+        sa.in = d_in;
+        sa.tv = tv;
+        sa.ginv = h->d_ginv;
+        sa.moduli = t->d_moduli;
+        sa.polys = batch * k_in;
+        sa.N = n;
+        sa.k_in = k_in;
+        sa.L = h->L;
+        sa.log_n = t->log_n;
+        scale_kernel<<<grid2(L * n, sa.polys), 256, 0, st>>>(sa);
+        count_launch();
+        PG_LAUNCH_CHECK("scale_kernel launch");
+        ModUpIO mio{};
+        mio.in = d_in;
+        mio.tv = tv;
+        mio.gmat = h->d_gmat;
+        mio.k_in = k_in;
+        mio.L = h->L;
+        mio.K = h->K;
+        mio.alpha = h->alpha;
+        mio.dnum = h->dnum;
+        mio.log_n = t->log_n;
+        int rc = launch_fused_ntt<MODE_FWD>(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, mio,
+                                            st);
+        if (rc) return rc;
+    } else {
+        int rc = modup(h, k_in, batch, d_in, ext, fp, st);
+        if (rc) return rc;
+        rc = launch_ntt(make_args(t, ext, batch * k_in * h->dnum * (L + K), 0), t->log_n, MODE_FWD, st);
+        if (rc) return rc;
+    }
     // sum over masks and groups, Q limbs to accq, P limbs to accp
-    rc = launch_mac(t, h->dnum, accq, nullptr, nullptr, d_key, ext, batch, k_in, (uint32_t)KO, 0, st, accp,
-                    h->L);
+    int rc = launch_mac(t, h->dnum, accq, nullptr, nullptr, d_key, ext, batch, k_in, (uint32_t)KO, 0, st, accp,
+                        h->L);
     if (rc) return rc;
+    if (fused) {
+        // ModDown with the P -> Q conversion and the final combination inside the transforms
+        PScaleIO pio{};
+        pio.accp = accp;
+        pio.pinv_k = h->d_pinv_k;
+        pio.K = h->K;
+        pio.log_n = t->log_n;
+        rc = launch_fused_ntt<MODE_INV>(make_args(&h->tp, accp, batch * KO * K, 0), t->log_n, pio, st);
+        if (rc) return rc;
+        PConvIO cio{};
+        cio.tvp = accp;
+        cio.pmat = h->d_pmat;
+        cio.bsrc = d_in + (size_t)k_in * L * n;  // b of ciphertext j: after its k_in masks
+        cio.bstride = (size_t)(k_in + 1) * L * n;
+        cio.accq = accq;
+        cio.pinv = h->d_pinv;
+        cio.out = d_out;
+        cio.K = h->K;
+        cio.L = h->L;
+        cio.ko = (uint32_t)KO;
+        cio.log_n = t->log_n;
+        // the rows' own storage is never touched: the policy loads and stores
+        return launch_fused_ntt<MODE_FWD>(make_args(&h->tq, conv, batch * KO * L, 0), t->log_n, cio, st);
+    }
     // ModDown: P limbs to coefficients, convert to Q, back to the NTT domain
     rc = launch_ntt(make_args(&h->tp, accp, batch * KO * K, 0), t->log_n, MODE_INV, st);
     if (rc) return rc;

@@ -758,8 +758,23 @@ PG_DEV void st_cluster(uint32_t local_addr, uint32_t rank, uint64_t v) {
 __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 / threads; }
 
 // One row of the cluster kernel: row u of the launch (see ntt_cluster_kernel).
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
-PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u) {
+// Where a forward transform of the cluster kernel takes its inputs and puts its
+// canonical outputs.  RowIO: the launch's rows (or, with NttArgs::lift_src, the
+// lifted gadget digits).  A policy with kLoad supplies the E inputs of a thread's
+// column itself, as values below 4q:
+//   template <int E> void load(p, limb, q, i0, stride, x[E])   x[jj] = input i0 + jj * stride
+// and one with kStore takes each canonical output of a forward or inverse
+// transform instead of the row store:
+//   void store(p, limb, q, i, v)
+// where p is the row's poly index (row = p * L + limb).  Fused producers and
+// consumers (the key switch's base conversions) use them to skip a pass
+// through HBM; the transform itself is unchanged.
+struct RowIO {
+    static constexpr bool kLoad = false, kStore = false;
+};
+
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, class IO = RowIO>
+PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const IO& io = IO{}) {
     constexpr bool FP = S == kSchedFp64;
     constexpr int KF = FP ? 2 : (S >= 1 ? 1 : 0), KI = FP ? 2 : (S >= 2 ? 1 : 0);  // round kinds
     constexpr bool FAST = KF == 1, FASTI = KI == 1;
@@ -798,12 +813,20 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u) {
         // matched by the wait before the first remote store; relaxed is enough
         // because this CTA has not touched shared memory yet
         cluster_arrive_relaxed();
-        const uint64_t* src = a.lift_src ? a.lift_src + (row / a.L) * N : g;  // digits to lift, or the row
+        if constexpr (IO::kLoad) {
+            static_assert(MODE == MODE_FWD, "a loading policy feeds forward transforms");
+            io.template load<E>(row / a.L, limb, q, gt, 1u << GX, x);
+        } else {
+            const uint64_t* src = a.lift_src ? a.lift_src + (row / a.L) * N : g;  // digits to lift, or the row
 #pragma unroll
-        for (int jj = 0; jj < E; ++jj) {
-            x[jj] = src[gt + (jj << GX)];
-            if (a.lift_src) x[jj] = lift_digit(x[jj], q, a.lift_basis, a.lift_half);
-            if constexpr (FP) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
+            for (int jj = 0; jj < E; ++jj) {
+                x[jj] = src[gt + (jj << GX)];
+                if (a.lift_src) x[jj] = lift_digit(x[jj], q, a.lift_basis, a.lift_half);
+            }
+        }
+        if constexpr (FP) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
         }
         fwd_round<LOG_N, LOG_E, GX, LOG_N - 1, GX, KF>(x, gt, 1, tw, mA, mB);
         cluster_wait_acquire();  // every CTA of the cluster is running
@@ -835,9 +858,15 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u) {
             __syncthreads();
             store_smem<LOG_E, 0>(x, sm, tid * E);
             __syncthreads();
-            uint64_t* gb = g + rank * M;
+            if constexpr (IO::kStore) {
+
 #pragma unroll
-            for (int k = 0; k < E; ++k) gb[tid + k * T] = sm[padi(tid + k * T)];
+                for (int k = 0; k < E; ++k) io.store(row / a.L, limb, q, rank * M + tid + k * T, sm[padi(tid + k * T)]);
+            } else {
+                uint64_t* gb = g + rank * M;
+#pragma unroll
+                for (int k = 0; k < E; ++k) gb[tid + k * T] = sm[padi(tid + k * T)];
+            }
         } else {
             const uint64_t* pv = a.plain + (size_t)limb * N + rank * M + tid * E;
             const uint64_t* pq = a.plain_q + (size_t)limb * N + rank * M + tid * E;
@@ -918,17 +947,23 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u) {
         for (int jj = 0; jj < E; ++jj) x[jj] = sm[padi((jj << LOG_T) + tid)];
         inv_round<LOG_N, LOG_N, LOG_E, GX, GX, LOG_N - 1, KI>(x, gt, 0, itw, (FP ? a.inv_n_fp : a.inv_n) + limb,
                                                               (FP ? a.inv_last_fp : a.inv_last) + limb, iA, iB, inv64);
+        if constexpr (IO::kStore) {
+            static_assert(MODE == MODE_INV, "a storing policy takes forward or inverse outputs");
 #pragma unroll
-        for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
+            for (int jj = 0; jj < E; ++jj) io.store(row / a.L, limb, q, gt + (jj << GX), x[jj]);
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
+        }
     }
 }
 
 // The cluster kernel: a grid of rows * C CTAs, one row per cluster of C CTAs.
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, class IO = RowIO>
 __global__ void __launch_bounds__(1 << (LOG_M - LOG_E), cluster_min_blocks(1 << (LOG_M - LOG_E)))
-    ntt_cluster_kernel(NttArgs a) {
+    ntt_cluster_kernel(NttArgs a, IO io) {
     extern __shared__ uint64_t smem_cl[];
-    cluster_row<LOG_N, LOG_M, LOG_E, MODE, S>(a, smem_cl, blockIdx.x >> (LOG_N - LOG_M));
+    cluster_row<LOG_N, LOG_M, LOG_E, MODE, S, IO>(a, smem_cl, blockIdx.x >> (LOG_N - LOG_M), io);
 }
 
 }  // namespace pg
@@ -958,11 +993,11 @@ static int launch_block(const NttArgs& a, cudaStream_t st) {
 // policy (each CTA of a cluster on its own SM).  Measured at N = 2^16, L = 24,
 // 128 polys: forward 1,761 -> 1,638 us, inverse 2,023 -> 1,923 us, round trip
 // unchanged; at N = 2^15 2-3% on every mode.
-template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S>
-static int launch_cluster(const NttArgs& a, cudaStream_t st, bool spread = false) {
+template <int LOG_N, int LOG_M, int LOG_E, int MODE, int S, class IO = RowIO>
+static int launch_cluster(const NttArgs& a, cudaStream_t st, bool spread = false, const IO& io = IO{}) {
     constexpr int C = 1 << (LOG_N - LOG_M), T = 1 << (LOG_M - LOG_E);
     constexpr size_t smem = (size_t)padded(1 << LOG_M) * sizeof(uint64_t);
-    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S>;
+    auto kern = ntt_cluster_kernel<LOG_N, LOG_M, LOG_E, MODE, S, IO>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return cuda_status(attr, "ntt_cluster_kernel: shared memory attribute");
     if (a.rows * C > 0x7fffffffull) return set_error(PG_ERR_UNSUPPORTED, "too many rows for one launch");
@@ -985,7 +1020,7 @@ static int launch_cluster(const NttArgs& a, cudaStream_t st, bool spread = false
         static const cudaError_t np = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (np != cudaSuccess) return cuda_status(np, "ntt_cluster_kernel: non-portable cluster size");
     }
-    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, io);
     count_launch();
     if (e != cudaSuccess) return cuda_status(e, "ntt_cluster_kernel launch");
     return PG_OK;
