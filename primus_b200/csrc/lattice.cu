@@ -71,7 +71,7 @@ struct MacArgs {
 // element once for the whole chunk, so a batch reads the digits once per pair
 // of output polys and the key ceil(B / kMacChunk) times.  Grid: x over
 // (chunk, output pair), y over 256-coefficient tiles (32-bit index).
-constexpr uint32_t kMacChunk = 2;
+constexpr uint32_t kMacChunk = 4;
 constexpr uint32_t kMacOut = 2;
 
 // NEG: the key-switch form (base - sum, base = add_last on the last output); SPLIT:
