@@ -123,7 +123,8 @@ __global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
 #pragma unroll
                 for (uint32_t cc = 0; cc < kMacOut; ++cc)
 #pragma unroll
-                    for (uint32_t bb = 0; bb < kMacChunk; ++bb) mac128(lo[cc][bb], hi[cc][bb], kv[cc], dv[bb]);
+                    for (uint32_t bb = 0; bb < kMacChunk; ++bb)
+                        if (bb < nb) mac128(lo[cc][bb], hi[cc][bb], kv[cc], dv[bb]);  // nb is uniform per CTA
             }
 #pragma unroll
             for (uint32_t cc = 0; cc < kMacOut; ++cc) {
