@@ -32,7 +32,7 @@ def _rank(rank, port, out):
 
 def test_max_over_ranks_gloo():
     port = _free_port()
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank, args=(port, out), nprocs=2, start_method="spawn", join=True)
     assert out[0] == out[1] == 2.5
 
