@@ -909,13 +909,19 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005, slots=4):
     srv.replay(reqs, np.cumsum(rng.exponential(1e6 / (2 * plain_rps), count)))
     srv.stats(reset=True)
 
+    kind_of = np.array([kind_names[it[0]] for it in trace])
+
     def summary(lat, wall, offered):
         ok = lat[lat >= 0]
+        # per kind: which requests make up the tail
+        p99_kind = {name: float(np.percentile(lat[(kind_of == name) & (lat >= 0)], 99))
+                    for name in kind_names.values() if ((kind_of == name) & (lat >= 0)).any()}
         return {"offered_rps": offered, "throughput_rps": len(ok) / wall, "p50_us": float(np.percentile(ok, 50)),
-                "p99_us": float(np.percentile(ok, 99)), "rejected": int((lat < 0).sum())}
+                "p99_us": float(np.percentile(ok, 99)), "p99_us_by_kind": p99_kind,
+                "rejected": int((lat < 0).sum())}
 
     plain_runs, served_runs = [], []
-    for mult in (0.5, 0.9, 2.0, 2.5, 3.0, 3.5, 4.0, 8.0, None):
+    for mult in (0.5, 0.9, 2.0, 2.5, 3.0, 3.25, 3.5, 3.75, 4.0, 8.0, None):
         offered = None if mult is None else plain_rps * mult
         arrivals = np.zeros(count) if mult is None else np.cumsum(rng.exponential(1e6 / offered, count))
         if mult is not None and mult < 1:
