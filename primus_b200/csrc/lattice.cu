@@ -65,8 +65,9 @@ struct MacArgs {
     int negate;
 };
 
-// One thread per (chunk of kMacChunk ciphertexts, pair of output polys, limb l,
-// coefficient x); lanes run over consecutive coefficients (coalesced).  Each
+// One thread per (chunk of kMacChunk ciphertexts -- one for a single ciphertext
+// --, pair of output polys, limb l, coefficient x); lanes run over consecutive
+// coefficients (coalesced).  Each
 // digit element is loaded once for both output polys of the pair and each key
 // element once for the whole chunk, so a batch reads the digits once per pair
 // of output polys and the key ceil(B / kMacChunk) times.  Grid: x over
@@ -77,11 +78,15 @@ constexpr uint32_t kMacOut = 2;
 // NEG: the key-switch form (base - sum, base = add_last on the last output); SPLIT:
 // limbs >= l_split written to out_hi (hybrid key switch).  Compile-time, so that
 // each launch carries only its own epilogue.
-template <bool FOLD, bool NEG, bool SPLIT>
+template <bool FOLD, bool NEG, bool SPLIT, uint32_t CHUNK>
 __global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
+    // terms whose key and digit loads are issued together: each thread has few
+    // terms (4 for a hybrid key switch), so one load round per term would leave
+    // the kernel waiting on memory latency instead of bandwidth
+    constexpr uint32_t U = CHUNK == 1 ? 4 : 1;
     const uint32_t LN = a.L * (uint32_t)a.N;
     const uint32_t pairs = (a.KOUT + kMacOut - 1) / kMacOut;
-    const size_t outer = ((a.B + kMacChunk - 1) / kMacChunk) * pairs;
+    const size_t outer = ((a.B + CHUNK - 1) / CHUNK) * pairs;
     const size_t kstride = (size_t)a.KOUT * LN;
     const size_t dstride = (size_t)a.KIN * a.d * LN;  // one ciphertext's digits
     const uint32_t nterms = a.KIN * a.d;
@@ -96,42 +101,54 @@ __global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
         for (size_t o = blockIdx.x; o < outer; o += gridDim.x) {
             const uint32_t c0 = (uint32_t)(o % pairs) * kMacOut;
             const uint32_t nc = min(kMacOut, a.KOUT - c0);
-            const size_t b0 = (o / pairs) * kMacChunk;
-            const uint32_t nb = (uint32_t)min((size_t)kMacChunk, a.B - b0);
-            uint64_t lo[kMacOut][kMacChunk], hi[kMacOut][kMacChunk];
+            const size_t b0 = (o / pairs) * CHUNK;
+            const uint32_t nb = (uint32_t)min((size_t)CHUNK, a.B - b0);
+            uint64_t lo[kMacOut][CHUNK], hi[kMacOut][CHUNK];
 #pragma unroll
             for (uint32_t cc = 0; cc < kMacOut; ++cc)
 #pragma unroll
-                for (uint32_t bb = 0; bb < kMacChunk; ++bb) lo[cc][bb] = hi[cc][bb] = 0;
+                for (uint32_t bb = 0; bb < CHUNK; ++bb) lo[cc][bb] = hi[cc][bb] = 0;
             const uint64_t* kp = a.key + (size_t)c0 * LN + lx;
             const uint64_t* dp = a.dig + b0 * dstride + lx;
-            for (uint32_t ij = 0; ij < nterms; ++ij) {
-                if (FOLD && ij && (ij & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
+            for (uint32_t ij0 = 0; ij0 < nterms; ij0 += U) {
+                uint64_t kv[U][kMacOut], dv[U][CHUNK];
+#pragma unroll
+                for (uint32_t u = 0; u < U; ++u) {
+                    const uint32_t ij = ij0 + u;
+                    const bool live = ij < nterms;
+#pragma unroll
+                    for (uint32_t cc = 0; cc < kMacOut; ++cc)
+                        kv[u][cc] = live && cc < nc ? __ldg(kp + ij * kstride + cc * LN) : 0;
+#pragma unroll
+                    for (uint32_t bb = 0; bb < CHUNK; ++bb)
+                        dv[u][bb] = live && bb < nb ? __ldg(dp + bb * dstride + ij * LN) : 0;
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < U; ++u) {
+                    const uint32_t ij = ij0 + u;
+                    if (ij >= nterms) break;
+                    if (FOLD && ij && (ij & 7) == 0) {  // products < 2^124: fold before the sum can reach 2^128
+#pragma unroll
+                        for (uint32_t cc = 0; cc < kMacOut; ++cc)
+#pragma unroll
+                            for (uint32_t bb = 0; bb < CHUNK; ++bb) {
+                                lo[cc][bb] = barrett_reduce_128(lo[cc][bb], hi[cc][bb], m);
+                                hi[cc][bb] = 0;
+                            }
+                    }
 #pragma unroll
                     for (uint32_t cc = 0; cc < kMacOut; ++cc)
 #pragma unroll
-                        for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
-                            lo[cc][bb] = barrett_reduce_128(lo[cc][bb], hi[cc][bb], m);
-                            hi[cc][bb] = 0;
-                        }
+                        for (uint32_t bb = 0; bb < CHUNK; ++bb)
+                            if (bb < nb) mac128(lo[cc][bb], hi[cc][bb], kv[u][cc], dv[u][bb]);  // nb is uniform per CTA
                 }
-                uint64_t kv[kMacOut], dv[kMacChunk];
-#pragma unroll
-                for (uint32_t cc = 0; cc < kMacOut; ++cc) kv[cc] = cc < nc ? __ldg(kp + ij * kstride + cc * LN) : 0;
-#pragma unroll
-                for (uint32_t bb = 0; bb < kMacChunk; ++bb) dv[bb] = bb < nb ? __ldg(dp + bb * dstride + ij * LN) : 0;
-#pragma unroll
-                for (uint32_t cc = 0; cc < kMacOut; ++cc)
-#pragma unroll
-                    for (uint32_t bb = 0; bb < kMacChunk; ++bb)
-                        if (bb < nb) mac128(lo[cc][bb], hi[cc][bb], kv[cc], dv[bb]);  // nb is uniform per CTA
             }
 #pragma unroll
             for (uint32_t cc = 0; cc < kMacOut; ++cc) {
                 if (cc >= nc) break;
                 const uint32_t c = c0 + cc;
 #pragma unroll
-                for (uint32_t bb = 0; bb < kMacChunk; ++bb) {
+                for (uint32_t bb = 0; bb < CHUNK; ++bb) {
                     if (bb >= nb) break;
                     const size_t b = b0 + bb;
                     const size_t bc = b * a.KOUT + c;
@@ -280,6 +297,25 @@ int digits_pipeline(const pg_ntt_table* t, const pg_gadget_basis* g, const uint6
 
 }  // namespace
 
+namespace {
+template <uint32_t CHUNK>
+void launch_mac_t(const MacArgs& a, uint32_t kout, size_t LN, bool fold, bool split, bool negate, cudaStream_t st) {
+    const size_t outer = ((a.B + CHUNK - 1) / CHUNK) * ((kout + kMacOut - 1) / kMacOut);
+    const dim3 grid((unsigned)std::min<size_t>(outer, 0x7fffffff),
+                    (unsigned)std::min<size_t>((LN + 255) / 256, 65535));
+    if (split) {
+        fold ? mac_kernel<true, false, true, CHUNK><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, false, true, CHUNK><<<grid, 256, 0, st>>>(a);
+    } else if (negate) {
+        fold ? mac_kernel<true, true, false, CHUNK><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, true, false, CHUNK><<<grid, 256, 0, st>>>(a);
+    } else {
+        fold ? mac_kernel<true, false, false, CHUNK><<<grid, 256, 0, st>>>(a)
+             : mac_kernel<false, false, false, CHUNK><<<grid, 256, 0, st>>>(a);
+    }
+}
+}  // namespace
+
 int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint64_t* acc, const uint64_t* add_last,
                    const uint64_t* key, const uint64_t* dig, size_t B, uint32_t kin, uint32_t kout, int negate,
                    cudaStream_t st, uint64_t* out_hi, uint32_t l_split) {
@@ -302,20 +338,13 @@ int pg::launch_mac(const pg_ntt_table* t, uint32_t d, uint64_t* out, const uint6
     a.negate = negate;
     if ((size_t)t->L * t->n > 0xffffffffull) return set_error(PG_ERR_UNSUPPORTED, "poly too large");
     const size_t LN = (size_t)t->L * t->n;
-    const size_t outer = ((B + kMacChunk - 1) / kMacChunk) * ((kout + kMacOut - 1) / kMacOut);
-    const dim3 grid((unsigned)std::min<size_t>(outer, 0x7fffffff),
-                    (unsigned)std::min<size_t>((LN + 255) / 256, 65535));
     const bool fold = kin * d > 8;  // more than 8 products per output: fold the 128-bit sums every 8
-    if (out_hi) {
-        if (negate) return set_error(PG_ERR_INVALID_ARGUMENT, "split MAC output has no key-switch form");
-        fold ? mac_kernel<true, false, true><<<grid, 256, 0, st>>>(a)
-             : mac_kernel<false, false, true><<<grid, 256, 0, st>>>(a);
-    } else if (negate) {
-        fold ? mac_kernel<true, true, false><<<grid, 256, 0, st>>>(a)
-             : mac_kernel<false, true, false><<<grid, 256, 0, st>>>(a);
+    if (out_hi && negate) return set_error(PG_ERR_INVALID_ARGUMENT, "split MAC output has no key-switch form");
+    // one ciphertext: the single-ciphertext form (fewer registers, more terms' loads in flight)
+    if (B == 1) {
+        launch_mac_t<1>(a, kout, LN, fold, out_hi != nullptr, negate != 0, st);
     } else {
-        fold ? mac_kernel<true, false, false><<<grid, 256, 0, st>>>(a)
-             : mac_kernel<false, false, false><<<grid, 256, 0, st>>>(a);
+        launch_mac_t<kMacChunk>(a, kout, LN, fold, out_hi != nullptr, negate != 0, st);
     }
     count_launch();
     PG_LAUNCH_CHECK("mac_kernel launch");
