@@ -400,9 +400,12 @@ struct PScaleIO {
     const ulonglong2* pinv_k;    // [K]
     uint32_t K, log_n;
 
-    PG_DEV void store(uint64_t p, uint32_t k, uint64_t q, uint32_t i, uint64_t v) const {
+    template <int E, class V>
+    PG_DEV void store(uint64_t p, uint32_t k, uint64_t q, uint32_t i0, uint32_t stride, V value) const {
         const ulonglong2 f = __ldg(pinv_k + k);
-        accp[((p * K + k) << log_n) + i] = shoup_mul(f.x, f.y, v, q);
+        uint64_t* dst = accp + ((p * K + k) << log_n) + i0;
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) dst[(size_t)jj * stride] = shoup_mul(f.x, f.y, value(jj), q);
     }
 };
 
@@ -441,10 +444,18 @@ struct PConvIO {
         }
     }
 
-    PG_DEV void store(uint64_t p, uint32_t l, uint64_t q, uint32_t i, uint64_t v) const {
-        const size_t idx = ((p * L + l) << log_n) + i;
+    template <int E, class V>
+    PG_DEV void store(uint64_t p, uint32_t l, uint64_t q, uint32_t i0, uint32_t stride, V value) const {
+        const size_t base = ((p * L + l) << log_n) + i0;
+        // every acc_Q load is issued before the first output store (out may
+        // alias acc_Q as far as the compiler knows, which would serialise them)
+        uint64_t acc[E];
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) acc[jj] = ld_stream(accq + base + (size_t)jj * stride);
         const ulonglong2 f = __ldg(pinv + l);
-        out[idx] = sub_mod(v, shoup_mul(f.x, f.y, ld_stream(accq + idx), q), q);
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj)
+            out[base + (size_t)jj * stride] = sub_mod(value(jj), shoup_mul(f.x, f.y, acc[jj], q), q);
     }
 };
 

@@ -763,10 +763,12 @@ __host__ __device__ constexpr int cluster_min_blocks(int threads) { return 1024 
 // lifted gadget digits).  A policy with kLoad supplies the E inputs of a thread's
 // column itself, as values below 4q:
 //   template <int E> void load(p, limb, q, i0, stride, x[E])   x[jj] = input i0 + jj * stride
-// and one with kStore takes each canonical output of a forward or inverse
-// transform instead of the row store:
-//   void store(p, limb, q, i, v)
-// where p is the row's poly index (row = p * L + limb).  Fused producers and
+// and one with kStore takes the canonical outputs of a thread's column of a
+// forward or inverse transform instead of the row store:
+//   template <int E, class V> void store(p, limb, q, i0, stride, V value)
+// output i0 + k * stride being value(k) for k < E (the policy may issue its own
+// loads for all E outputs before it reads the values), where p is the row's
+// poly index (row = p * L + limb).  Fused producers and
 // consumers (the key switch's base conversions) use them to skip a pass
 // through HBM; the transform itself is unchanged.
 struct RowIO {
@@ -859,9 +861,8 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const 
             store_smem<LOG_E, 0>(x, sm, tid * E);
             __syncthreads();
             if constexpr (IO::kStore) {
-
-#pragma unroll
-                for (int k = 0; k < E; ++k) io.store(row / a.L, limb, q, rank * M + tid + k * T, sm[padi(tid + k * T)]);
+                io.template store<E>(row / a.L, limb, q, rank * M + tid, T,
+                                     [&](int k) { return sm[padi(tid + k * T)]; });
             } else {
                 uint64_t* gb = g + rank * M;
 #pragma unroll
@@ -949,8 +950,7 @@ PG_DEV void cluster_row(const NttArgs& a, uint64_t* sm, const uint64_t u, const 
                                                               (FP ? a.inv_last_fp : a.inv_last) + limb, iA, iB, inv64);
         if constexpr (IO::kStore) {
             static_assert(MODE == MODE_INV, "a storing policy takes forward or inverse outputs");
-#pragma unroll
-            for (int jj = 0; jj < E; ++jj) io.store(row / a.L, limb, q, gt + (jj << GX), x[jj]);
+            io.template store<E>(row / a.L, limb, q, gt, 1u << GX, [&](int jj) { return x[jj]; });
         } else {
 #pragma unroll
             for (int jj = 0; jj < E; ++jj) g[gt + (jj << GX)] = x[jj];
