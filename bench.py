@@ -777,7 +777,7 @@ def run_workload(args):
     fn = {"polymul_n1024": lambda: bench_polymul_1024(P, stream),
           "uneven_batch": lambda: bench_uneven(P, stream),
           "ext_product": lambda: bench_ext_product(P, stream, cpu=not args.no_cpu),
-          "hybrid_ks": lambda: bench_hybrid_ks(P, stream),
+          "hybrid_ks": lambda: bench_hybrid_ks(P, stream, batches=tuple(args.ks_batches)),
           "widened": lambda: bench_widened(P, stream),
           "pointwise": lambda: bench_pointwise(P, stream),
           "expand": lambda: bench_expand(P, stream, cpu=not args.no_cpu),
@@ -965,6 +965,8 @@ def main(argv=None):
                     choices=["polymul_n1024", "uneven_batch", "ext_product", "hybrid_ks", "widened",
                              "pointwise", "expand", "served_mixed", "autotune_L24"],
                     help="run only this secondary workload and print its result")
+    ap.add_argument("--ks-batches", type=int, nargs="+", default=[1, 8, 32],
+                    help="key switches per call timed by --workload hybrid_ks")
     args = ap.parse_args(argv)
     set_polys(args.polys)
     if args.workload:

@@ -79,7 +79,7 @@ constexpr uint32_t kMacOut = 2;
 // limbs >= l_split written to out_hi (hybrid key switch).  Compile-time, so that
 // each launch carries only its own epilogue.
 template <bool FOLD, bool NEG, bool SPLIT, uint32_t CHUNK>
-__global__ void __launch_bounds__(256, 3) mac_kernel(MacArgs a) {
+__global__ void __launch_bounds__(256, CHUNK == 1 ? 4 : 3) mac_kernel(MacArgs a) {
     // terms whose key and digit loads are issued together: each thread has few
     // terms (4 for a hybrid key switch), so one load round per term would leave
     // the kernel waiting on memory latency instead of bandwidth
