@@ -529,12 +529,20 @@ HybridWs hybrid_ws(const pg_hybrid_ks* h, uint32_t k_in, uint32_t k_out, size_t 
 }
 
 // the fused transforms run the cluster kernel's default shape of each degree
+constexpr uint64_t kFusedNarrowRows = 32;
+
 template <int MODE, class IO>
 int launch_fused_ntt(const NttArgs& a, uint32_t log_n, const IO& io, cudaStream_t st) {
     switch (log_n) {
         case 13: return launch_cluster<13, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
         case 14: return launch_cluster<14, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
-        case 15: return launch_cluster<15, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
+        case 15:
+            // a launch of a few rows (a single key switch's P rows and converted
+            // rows) runs 8 elements per thread: twice the threads per row, so each
+            // thread's chain of loads and butterflies is half as long, and all of
+            // its clusters still fit one wave (2 CTAs of 512 threads per SM)
+            if (a.rows <= kFusedNarrowRows) return launch_cluster<15, 12, 3, MODE, kSchedFp64, IO>(a, st, false, io);
+            return launch_cluster<15, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
         case 16: return launch_cluster<16, 12, 4, MODE, kSchedFp64, IO>(a, st, false, io);
     }
     return set_error(PG_ERR_UNSUPPORTED, "fused key switch: ring degree outside 2^13 .. 2^16");

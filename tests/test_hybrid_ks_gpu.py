@@ -12,12 +12,13 @@ pytestmark = pytest.mark.gpu
 
 
 # (log_n, L, K, alpha, k_in, k_out, batch): the served shape (N=2^15, L=16, K=4,
-# 4-limb groups), a ragged last group, a single group, and larger k
+# 4-limb groups) in batches of 2 and 1, a ragged last group, a single group, and larger k
 # (N = 2^13 .. 2^16 and batches of at most 8 run the fused form: conversions inside
-# the transforms' loads and stores; smaller N and larger batches the separate kernels)
-SHAPES = [(15, 16, 4, 4, 1, 1, 2), (10, 7, 2, 3, 1, 1, 3), (11, 4, 1, 4, 1, 1, 2), (10, 6, 3, 2, 2, 2, 2),
-          (12, 5, 2, 1, 1, 3, 1), (13, 6, 2, 3, 2, 1, 2), (14, 7, 3, 2, 1, 2, 3), (16, 5, 1, 4, 1, 1, 1),
-          (13, 4, 2, 2, 1, 1, 9)]
+# the transforms' loads and stores; smaller N and larger batches the separate kernels;
+# at N = 2^15 fused launches of at most 32 rows run 8 elements per thread)
+SHAPES = [(15, 16, 4, 4, 1, 1, 2), (15, 16, 4, 4, 1, 1, 1), (10, 7, 2, 3, 1, 1, 3), (11, 4, 1, 4, 1, 1, 2),
+          (10, 6, 3, 2, 2, 2, 2), (12, 5, 2, 1, 1, 3, 1), (13, 6, 2, 3, 2, 1, 2), (14, 7, 3, 2, 1, 2, 3),
+          (16, 5, 1, 4, 1, 1, 1), (13, 4, 2, 2, 1, 1, 9)]
 
 
 @pytest.mark.parametrize("log_n,L,K,alpha,k_in,k_out,batch", SHAPES)
