@@ -48,11 +48,17 @@ PG_DEV void decompose_word(uint64_t v, const GadgetWord& g, DT* dst) {
     }
 }
 
-template <int LOG_N, int LOG_E, typename DT, bool FAST>
-__global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFusedArgs a) {
+// TAB (small bases, fast forward schedule): the first forward stage pairs element
+// i with i + N/2 under the one twiddle w = root_powers[1], and its product operand
+// is a lifted digit, one of `basis` values, so the products w * lift(digit) mod q
+// come from a table of `basis` words in shared memory instead of Shoup products.
+template <int LOG_N, int LOG_E, typename DT, bool FAST, bool TAB>
+__global__ void __launch_bounds__(1 << (LOG_N - LOG_E), LOG_N == 11 ? 2 : 1) ext_fused_kernel(ExtFusedArgs a) {
     constexpr int N = 1 << LOG_N, E = 1 << LOG_E, T = N / E, KP = 2;
+    static_assert(!TAB || FAST, "the table form feeds the fast forward schedule");
     extern __shared__ uint64_t smem_ext[];
     // shared memory: NTT exchange buffer | 128-bit accumulators [KP][E][T] | digits [d][N]
+    // | (TAB) first-stage products [basis]
     uint64_t* sm = smem_ext;
     ulonglong2* acc = reinterpret_cast<ulonglong2*>(smem_ext + padded(N));
     DT* dg = reinterpret_cast<DT*>(acc + KP * N);
@@ -62,8 +68,18 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
     const uint64_t q = bar.q, q2 = q << 1, nq = 0 - q;
     const uint32_t d = a.gw.d;
     const uint64_t basis = a.gw.basis, half = (basis + 1) / 2, lift = q - basis;
+    uint64_t* tab = reinterpret_cast<uint64_t*>(dg + (size_t)d * N);
+    if constexpr (TAB) {
+        const ulonglong2 w1 = a.fwd[1];
+        for (uint32_t v = tid; v < basis; v += T) {
+            const uint64_t lv = (basis == 2 || v < half) ? v : lift + v;
+            tab[v] = shoup_mul(w1.x, w1.y, lv, q);
+        }
+        __syncthreads();
+    }
     using R0 = FwdRounds<LOG_N, LOG_E, 0>;
     static_assert(R0::G == LOG_N - LOG_E, "first forward group is the column tid + jj*T");
+    static_assert(!TAB || R0::P_HI > R0::P_LO, "the table stage leaves at least one stage in the first round");
     // each thread owns accumulator entries (c, e, tid): no other thread touches them
 #pragma unroll
     for (int ce = 0; ce < KP * E; ++ce) acc[ce * T + tid] = make_ulonglong2(0, 0);
@@ -79,12 +95,26 @@ __global__ void __launch_bounds__(1 << (LOG_N - LOG_E)) ext_fused_kernel(ExtFuse
         for (int jj = 0; jj < E; ++jj) decompose_word<DT, N>(v[jj], a.gw, dg + tid + jj * T);
         for (uint32_t j = 0; j < d; ++j) {
             uint64_t x[E];
+            if constexpr (TAB) {
+                // stage LOG_N - 1: (u + w y, u - w y) with w y = tab[digit of y], u = the
+                // lifted digit of x; outputs below 2q, inside the fast schedule's bounds
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) {
-                const uint64_t v = dg[(size_t)j * N + tid + jj * T];
-                x[jj] = (basis == 2 || v < half) ? v : lift + v;  // wrapping_decompose_small_values
+                for (int jj = 0; jj < E / 2; ++jj) {
+                    const uint64_t v = dg[(size_t)j * N + tid + jj * T];
+                    const uint64_t u = (basis == 2 || v < half) ? v : lift + v;
+                    const uint64_t t = tab[dg[(size_t)j * N + tid + (jj + E / 2) * T]];
+                    x[jj] = u + t;
+                    x[jj + E / 2] = u + q - t;
+                }
+                fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI - 1, R0::P_LO, FAST>(x, tid, 1, a.fwd, q2, nq);
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) {
+                    const uint64_t v = dg[(size_t)j * N + tid + jj * T];
+                    x[jj] = (basis == 2 || v < half) ? v : lift + v;  // wrapping_decompose_small_values
+                }
+                fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, a.fwd, q2, nq);
             }
-            fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, FAST>(x, tid, 1, a.fwd, q2, nq);
             __syncthreads();  // the previous row's last shared-memory reads are done
             fwd_rest<LOG_N, LOG_N, LOG_E, 1, FAST>(x, sm, tid, 1, a.fwd, q2, nq);
             if constexpr (!FAST) {
@@ -193,10 +223,10 @@ static int launch_mode(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
 // the opt-in maximum of dynamic shared memory per CTA on sm_100 (227 KiB)
 constexpr size_t kExtFusedMaxSmem = 227 * 1024;
 
-template <int LOG_N, int LOG_E, typename DT, bool FAST>
+template <int LOG_N, int LOG_E, typename DT, bool FAST, bool TAB>
 static int launch_ext_fused_t(const ExtFusedArgs& a, size_t smem, cudaStream_t st) {
     constexpr int T = 1 << (LOG_N - LOG_E);
-    auto kern = ext_fused_kernel<LOG_N, LOG_E, DT, FAST>;
+    auto kern = ext_fused_kernel<LOG_N, LOG_E, DT, FAST, TAB>;
     // shared memory grows with the digit count; raise the limit to the largest allowed once
     static const cudaError_t attr =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kExtFusedMaxSmem);
@@ -207,20 +237,28 @@ static int launch_ext_fused_t(const ExtFusedArgs& a, size_t smem, cudaStream_t s
     return PG_OK;
 }
 
-template <typename DT, bool FAST>
+template <typename DT, bool FAST, bool TAB = false>
 static int launch_ext_fused_n(const ExtFusedArgs& a, uint32_t log_n, size_t smem, cudaStream_t st) {
     switch (log_n) {
-        case 10: return launch_ext_fused_t<10, 3, DT, FAST>(a, smem, st);
+        case 10: return launch_ext_fused_t<10, 3, DT, FAST, TAB>(a, smem, st);
         // 2^11: E = 4 (512 threads, 64 registers, two CTAs per SM) beats E = 8 by 4.5%
-        case 11: return launch_ext_fused_t<11, 2, DT, FAST>(a, smem, st);
-        case 12: return launch_ext_fused_t<12, 3, DT, FAST>(a, smem, st);
+        case 11: return launch_ext_fused_t<11, 2, DT, FAST, TAB>(a, smem, st);
+        case 12: return launch_ext_fused_t<12, 3, DT, FAST, TAB>(a, smem, st);
         default: return set_error(PG_ERR_UNSUPPORTED, "fused external product: log_n outside 10..12");
     }
 }
 
+// first-stage product tables for bases up to this size (2 KiB of shared memory)
+constexpr uint64_t kExtTabMaxBasis = 256;
+
+static bool ext_fused_tab(const pg_ntt_table* t, const GadgetWord& gw) {
+    return gw.basis <= kExtTabMaxBasis && gw.log_basis <= 16 && t->moduli[0] < (1ull << 58);
+}
+
 static size_t ext_fused_smem(const pg_ntt_table* t, const GadgetWord& gw) {
     const size_t dt = gw.log_basis <= 16 ? 2 : 8;
-    return (size_t)padded((int)t->n) * 8 + 2 * t->n * 16 + (size_t)gw.d * t->n * dt;
+    return (size_t)padded((int)t->n) * 8 + 2 * t->n * 16 + (size_t)gw.d * t->n * dt +
+           (ext_fused_tab(t, gw) ? gw.basis * 8 : 0);
 }
 
 bool ext_fused_eligible(const pg_ntt_table* t, const GadgetWord& gw, uint32_t k) {
@@ -247,6 +285,7 @@ int launch_ext_fused(const pg_ntt_table* t, const GadgetWord& gw, const uint64_t
     a.out_coeff = out_coeff ? 1 : 0;
     const size_t smem = ext_fused_smem(t, gw);
     const bool fast = t->moduli[0] < (1ull << 58);
+    if (ext_fused_tab(t, gw)) return launch_ext_fused_n<uint16_t, true, true>(a, t->log_n, smem, st);
     if (gw.log_basis <= 16)
         return fast ? launch_ext_fused_n<uint16_t, true>(a, t->log_n, smem, st)
                     : launch_ext_fused_n<uint16_t, false>(a, t->log_n, smem, st);
