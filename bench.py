@@ -921,7 +921,7 @@ def bench_served(P, stream, count=2000, seed=0x5EED0005, slots=4):
                 "rejected": int((lat < 0).sum())}
 
     plain_runs, served_runs = [], []
-    for mult in (0.5, 0.9, 2.0, 2.5, 3.0, 3.25, 3.5, 3.75, 4.0, 8.0, None):
+    for mult in (0.5, 0.9, 2.0, 2.25, 2.5, 2.75, 3.0, 3.25, 3.5, 3.75, 4.0, 8.0, None):
         offered = None if mult is None else plain_rps * mult
         arrivals = np.zeros(count) if mult is None else np.cumsum(rng.exponential(1e6 / offered, count))
         if mult is not None and mult < 1:

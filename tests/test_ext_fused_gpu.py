@@ -21,9 +21,12 @@ def _setup(log_n, q, lb):
 # (log_n, modulus bound, log_basis, batch): the blind-rotation shape (2^11, q < 2^54,
 # 7-bit digits), 16-bit digits, wide digits kept as 64-bit words, a modulus above
 # 2^58 (lazy Harvey forward schedule), and base 2 (many digits, many folds)
-# (the fused kernel runs for batches of 64 and more; the batch of 5 takes the pipeline)
+# (the fused kernel runs for batches of 64 and more; the batch of 5 takes the pipeline;
+# bases up to 256 below 2^58 take the first forward stage from a table: the largest
+# table at N = 2^12, and a modulus just below 2^58)
 SHAPES = [(11, 1 << 54, 7, 100), (10, 1 << 54, 7, 5), (10, 1 << 54, 7, 64), (12, 1 << 50, 10, 65),
-          (11, 1 << 50, 16, 64), (11, 1 << 54, 20, 70), (11, 1 << 61, 16, 64), (10, 1 << 40, 1, 64)]
+          (11, 1 << 50, 16, 64), (11, 1 << 54, 20, 70), (11, 1 << 61, 16, 64), (10, 1 << 40, 1, 64),
+          (12, 1 << 50, 8, 64), (11, 1 << 58, 6, 64)]
 
 
 @pytest.mark.parametrize("log_n,bound,lb,batch", SHAPES)
