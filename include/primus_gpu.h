@@ -511,7 +511,8 @@ int pg_key_switch_hybrid(const pg_hybrid_ks *ks, uint32_t k_in, uint32_t k_out, 
  * transform_slice x2, mul_assign, inverse_transform_slice
  * (primus_ntt/src/ntt/primitive.rs:234-296, primus_poly/src/dcrt/mul.rs:97-110).
  * One run launches, per ring degree present, a forward NTT over every a- and
- * b-row and a fused multiply + inverse NTT over every a-row, the degrees on
+ * b-row and a fused multiply + inverse NTT over every a-row (for N <= 2^12 with
+ * every modulus below 2^50, one launch doing both per row), the degrees on
  * parallel streams.  With use_graph the first run of a job shape is captured
  * into a CUDA graph and later runs of the same shape replay it. */
 typedef struct pg_polymul_job {

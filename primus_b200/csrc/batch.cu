@@ -9,6 +9,9 @@
 // Schedule: jobs are grouped by ring degree.  Each degree class gets two
 // descriptor-driven launches: one forward NTT over every a- and b-row of the
 // class, then one fused (multiply by the b-row, inverse NTT) over every a-row.
+// Classes of N <= 2^12 on the FP64 schedule take one launch instead, whose CTAs
+// transform the b-row, then the a-row, multiply and run the inverse (the pair
+// form of the block kernel).
 // Rows are listed limb-major so that concurrently running CTAs share a prime's
 // twiddles.  The classes run on forked streams, and the whole set of launches
 // is captured once into a CUDA graph that later calls replay (a job set with
@@ -72,6 +75,17 @@ bool same_plan(const std::vector<pg_polymul_batch::Cls>& x, const std::vector<pg
     return true;
 }
 
+// kernel launches of the last call's plan: one per class in the pair form, else two
+size_t plan_launches(const pg_polymul_batch* b) {
+    size_t n = 0;
+    for (const auto& c : b->plan) {
+        NttArgs ia = make_args(b->tables[c.log_n], nullptr, c.inv_n, 0);
+        ia.desc = b->d_desc + c.inv_off;
+        n += pair_ok(ia, (uint32_t)c.log_n) ? 1 : 2;
+    }
+    return n;
+}
+
 // the per-class launches, forked off `st` and joined back into it (a batch of
 // one ring degree runs on `st` itself: no cross-stream dependencies to pay for)
 int enqueue(pg_polymul_batch* b, cudaStream_t st) {
@@ -81,13 +95,20 @@ int enqueue(pg_polymul_batch* b, cudaStream_t st) {
         cudaStream_t cs = fork ? b->streams[c.log_n] : st;
         if (fork) PG_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
         const pg_ntt_table* t = b->tables[c.log_n];
-        NttArgs fa = make_args(t, nullptr, c.fwd_n, 0);
-        fa.desc = b->d_desc + c.fwd_off;
-        int rc = launch_ntt(fa, t->log_n, MODE_FWD, cs);
-        if (rc) return rc;
         NttArgs ia = make_args(t, nullptr, c.inv_n, 0);
         ia.desc = b->d_desc + c.inv_off;
-        rc = launch_ntt(ia, t->log_n, MODE_INV, cs);
+        int rc;
+        if (pair_ok(ia, t->log_n)) {
+            // one CTA transforms b, multiplies and runs the inverse of a: one launch,
+            // and a's forward never goes through HBM
+            rc = launch_pair(ia, t->log_n, cs);
+        } else {
+            NttArgs fa = make_args(t, nullptr, c.fwd_n, 0);
+            fa.desc = b->d_desc + c.fwd_off;
+            rc = launch_ntt(fa, t->log_n, MODE_FWD, cs);
+            if (rc) return rc;
+            rc = launch_ntt(ia, t->log_n, MODE_INV, cs);
+        }
         if (rc) return rc;
         if (fork) {
             PG_CUDA(cudaEventRecord(b->joins[c.log_n], cs));
@@ -235,7 +256,7 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
     }
     if (b->exec && same_plan(b->plan, b->graph_plan) && b->graph_desc == b->d_desc) {
         PG_CUDA(cudaGraphLaunch(b->exec, st));
-        count_launch(2 * b->plan.size());
+        count_launch(plan_launches(b));
         PG_CUDA(cudaEventRecord(b->finished, st));
         return PG_OK;
     }

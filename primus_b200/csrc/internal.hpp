@@ -115,7 +115,7 @@ namespace pg {
 // applied before the transform
 struct RowDesc {
     uint64_t* data;
-    const uint64_t* mul;
+    uint64_t* mul;  // NTT-domain multiplicand (read); the pair form transforms it in place
     uint32_t limb;
     uint32_t pad;
 };
@@ -150,7 +150,9 @@ struct NttArgs {
     int variant[3];  // kernel shape per mode (0 = default), chosen by the autotuner
 };
 
-enum NttMode { MODE_FWD = 0, MODE_INV = 1, MODE_RT = 2 };
+// MODE_PAIR (descriptor rows, block kernel, FP64 schedule): per row b <- NTT(b)
+// and a <- INTT(NTT(a) * NTT(b)) in one pass, b being the descriptor's multiplicand
+enum NttMode { MODE_FWD = 0, MODE_INV = 1, MODE_RT = 2, MODE_PAIR = 3 };
 
 // one gadget digit's window in the BigUint value: bits [shr, ...) of limb
 // `index`, continued by `mask1` bits of limb index + 1 when the digit straddles
@@ -202,6 +204,11 @@ inline NttArgs make_args(const pg_ntt_table* t, uint64_t* data, uint64_t rows, i
 }
 
 int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t stream);
+// the pair form over descriptor rows (log_n <= kPairMaxLogN, every modulus below
+// 2^50 with FP64 tables): one launch instead of a forward and an inverse one
+constexpr uint32_t kPairMaxLogN = 12;
+bool pair_ok(const NttArgs& a, uint32_t log_n);
+int launch_pair(const NttArgs& a, uint32_t log_n, cudaStream_t stream);
 // alternative kernel shapes (ntt_variants.cu): variant 1 .. ntt_variant_count(log_n) - 1
 // of the canonical forward, the inverse and the round trip; identical results
 int ntt_variant_count(uint32_t log_n);

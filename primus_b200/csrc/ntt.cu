@@ -324,6 +324,33 @@ int launch_ntt(const NttArgs& a, uint32_t log_n, int mode, cudaStream_t st) {
     return set_error(PG_ERR_INVALID_ARGUMENT, "bad NTT mode");
 }
 
+bool pair_ok(const NttArgs& a, uint32_t log_n) {
+    return log_n >= 1 && log_n <= kPairMaxLogN && a.desc && fast_inv_ok(a) && a.fwd_fp;
+}
+
+// the default block shapes of launch_mode, in the pair form
+int launch_pair(const NttArgs& a, uint32_t log_n, cudaStream_t st) {
+    if (a.rows == 0) return PG_OK;
+    if (!pair_ok(a, log_n)) return set_error(PG_ERR_UNSUPPORTED, "pair form: needs descriptor rows, log_n <= 12 "
+                                                                 "and every modulus below 2^50");
+    constexpr int M = MODE_PAIR, S = kSchedFp64;
+    switch (log_n) {
+        case 1: return launch_block<1, 1, 128, M, S>(a, st);
+        case 2: return launch_block<2, 2, 128, M, S>(a, st);
+        case 3: return launch_block<3, 3, 128, M, S>(a, st);
+        case 4: return launch_block<4, 3, 64, M, S>(a, st);
+        case 5: return launch_block<5, 3, 32, M, S>(a, st);
+        case 6: return launch_block<6, 3, 16, M, S>(a, st);
+        case 7: return launch_block<7, 3, 8, M, S>(a, st);
+        case 8: return launch_block<8, 3, 4, M, S>(a, st);
+        case 9: return launch_block<9, 3, 2, M, S>(a, st);
+        case 10: return launch_block<10, 3, 1, M, S>(a, st);
+        case 11: return launch_block<11, 3, 1, M, S>(a, st);
+        case 12: return launch_block<12, 4, 1, M, S>(a, st);
+    }
+    return set_error(PG_ERR_UNSUPPORTED, "pair form: log_n outside 1..12");
+}
+
 // ---------------------------------------------------------------- monomials
 // transform_monomial (primus_ntt/src/ntt/primitive.rs:298-349): out[i] =
 // coeff * psi^((2 rev(i) + 1) * degree mod 2N); kind 0 = general coeff,

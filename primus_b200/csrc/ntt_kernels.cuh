@@ -617,7 +617,7 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     const uint64_t row = active ? (u % polys) * a.L + limb : 0;
     uint64_t* sm = smem_block + threadIdx.y * padded(N);
     uint64_t* g = a.data + row * N;
-    const uint64_t* mulp = nullptr;
+    uint64_t* mulp = nullptr;  // descriptor multiplicand (the pair form's b row)
     if (a.desc) {  // descriptor-driven rows (ragged batches)
         const RowDesc d = a.desc[active ? u : 0];
         g = d.data;
@@ -629,8 +629,35 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
     // the rounds' modulus words: (2q, -q) on the integer schedules, (q, 1/q) as doubles on FP64
     const uint64_t mA = FP ? as_u(fm.q) : q2, mB = FP ? as_u(fm.qinv) : nq;
     uint64_t x[E];
+    uint64_t xb[E];  // (pair form) NTT(b), canonical: elements tid*E .. tid*E+E-1
 
-    if constexpr (MODE == MODE_FWD || MODE == MODE_RT) {
+    if constexpr (MODE == MODE_PAIR) {
+        static_assert(FP, "the pair form runs on the FP64 schedule");
+        // b <- NTT(b): the forward of the multiplicand row, kept in registers for
+        // the product and stored back in place (coalesced, through smem)
+        const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
+        using R0 = FwdRounds<LOG_N, LOG_E, 0>;
+        uint64_t* bp = mulp;  // every pair descriptor carries its b row
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) {
+            x[jj] = active ? bp[tid + jj * T] : 0;
+            x[jj] = as_u(freduce(u52_to_f(x[jj]), fm.q, fm.qinv));  // inputs < 4q < 2^52
+        }
+        fwd_round<LOG_N, LOG_E, R0::G, R0::P_HI, R0::P_LO, KF>(x, tid, 1, tw, mA, mB);
+        fwd_rest<LOG_N, LOG_N, LOG_E, 1, KF>(x, sm, tid, 1, tw, mA, mB);
+#pragma unroll
+        for (int jj = 0; jj < E; ++jj) xb[jj] = f_to_u52(fcanon(freduce(as_f(x[jj]), fm.q, fm.qinv), fm.q));
+        __syncthreads();
+        store_smem<LOG_E, 0>(xb, sm, tid * E);
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < E; ++k) bp[tid + k * T] = sm[padi(tid + k * T)];
+        }
+        __syncthreads();  // every read of the exchange buffer is done before a's rounds
+    }
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_RT || MODE == MODE_PAIR) {
         const auto* tw = fwd_table<FP>(a) + (size_t)limb * N;
         using R0 = FwdRounds<LOG_N, LOG_E, 0>;
         // round 0 reads the row straight from HBM: x[jj] = row[tid + jj*T] (or the
@@ -663,6 +690,14 @@ __global__ void __launch_bounds__((1 << (LOG_N - LOG_E)) * ROWS) ntt_block_kerne
             if (active) {
 #pragma unroll
                 for (int k = 0; k < E; ++k) g[tid + k * T] = sm[padi(tid + k * T)];
+            }
+        } else if constexpr (MODE == MODE_PAIR) {
+            // x * NTT(b): w canonical, wq = w * (1/q) within 2^-52 relative of w/q, so the
+            // product of |x| < 2q + 2 lands in [-q, q] (a valid inverse input)
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) {
+                const double w = u52_to_f(xb[jj]);
+                x[jj] = as_u(fmulmod(as_f(x[jj]), w, __dmul_rn(w, fm.qinv), fm.q));
             }
         } else {
             // pointwise product with the NTT-domain plaintext (Shoup-prepared);

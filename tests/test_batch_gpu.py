@@ -17,9 +17,9 @@ def make_jobs(seed, count, log_ns, max_L, rng):
     return jobs
 
 
-def run_case(gpu, log_ns, max_L, count, seed, graph_reps=3):
+def run_case(gpu, log_ns, max_L, count, seed, graph_reps=3, bound=1 << 50):
     rng = np.random.default_rng(seed)
-    primes = {ln: O.ntt_primes(1 << 50, 2 << ln, max_L) for ln in log_ns}
+    primes = {ln: O.ntt_primes(bound, 2 << ln, max_L) for ln in log_ns}
     tables = {ln: gpu.DcrtTable(ln, primes[ln]) for ln in log_ns}
     refs = {ln: O.DcrtTable(ln, primes[ln]) for ln in log_ns}
     batch = gpu.PolymulBatch(list(tables.values()))
@@ -52,6 +52,16 @@ def test_uneven_small(gpu):
 
 def test_uneven_cluster_sizes(gpu):
     run_case(gpu, [10, 13, 14, 15, 16], 4, 12, seed=2, graph_reps=2)
+
+
+def test_uneven_tiny_degrees(gpu):
+    # N <= 2^12 with moduli below 2^50: one launch per degree (the pair form), several rows per CTA
+    run_case(gpu, [1, 2, 3, 5, 6, 8, 9, 12], 3, 24, seed=3, graph_reps=2)
+
+
+def test_uneven_wide_moduli(gpu):
+    # moduli above 2^50 (no FP64 schedule): the forward and the fused inverse launches
+    run_case(gpu, [3, 10, 12, 14], 3, 12, seed=4, graph_reps=2, bound=1 << 62)
 
 
 def test_single_job_plain_form(gpu):
