@@ -403,6 +403,29 @@ def run_gpu(args):
     e2e_ms = dist_max(dist, e0.elapsed_ms(e1) / e2e_steps, local)
     check.check("end to end through the host-slice call", rounds + 2 + e2e_steps,
                 lambda row: host[row * N:(row + 1) * N].copy())
+    # the host link of this box: the step's H2D and D2H bytes as two concurrent copies
+    # on two streams with no kernels (one cudaMemcpyAsync each); the end-to-end leg
+    # cannot run faster than this
+    hp2 = C.c_void_p()
+    nat.call("pg_host_alloc", C.byref(hp2), nbytes)
+    dev2 = P.DeviceBuffer(POLYS * L * N)
+    s2, ea, eb = P.Stream(), P.Event(), P.Event()
+    link_runs = []
+    for _ in range(3):
+        stream.synchronize()
+        s2.synchronize()
+        e0.record(stream)
+        nat.call("pg_memcpy_h2d", dev2.ptr, hp.value, nbytes, stream.h)
+        nat.call("pg_memcpy_d2h", hp2.value, data.ptr, nbytes, s2.h)
+        ea.record(stream)
+        eb.record(s2)
+        stream.synchronize()
+        s2.synchronize()
+        link_runs.append(max(e0.elapsed_ms(ea), e0.elapsed_ms(eb)))
+    link_ms = min(link_runs)
+    nat.call("pg_host_free", hp2.value)
+    del dev2
+    s2.close()
     nat.call("pg_host_free", hp.value)
     e2e_value = NTT_PER_STEP * world / (e2e_ms / 1e3)
 
@@ -467,7 +490,9 @@ def run_gpu(args):
                                                     for k in ('forward', 'inverse', 'round_trip')) + ")"),
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                    "ms_per_step": e2e_ms, "path": "pg_dcrt_polymul_ntt_plain_host (pinned host slice; chunked H2D / fused launch / D2H on 3 streams)"},
+                    "ms_per_step": e2e_ms, "path": "pg_dcrt_polymul_ntt_plain_host (pinned host slice; chunked H2D / fused launch / D2H on 3 streams)",
+                    "host_link_ms_per_step": link_ms, "frac_of_host_link": link_ms / e2e_ms,
+                    "host_link_note": "the same H2D and D2H bytes as two concurrent copies, no kernels (this box)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,
