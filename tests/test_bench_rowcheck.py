@@ -16,18 +16,24 @@ def test_rowcheck_rows_follow_whole_poly_round_trips():
     rc = bench.RowCheck(moduli, seed, threads=8)
     full = O.DcrtTable(bench.LOG_N, moduli)
     plain = full.forward(O.uniform_rns(bench.SEED + 7, 0, moduli, bench.N), threads=8)
-    rows = {}
+    rows, rows1 = {}, {}
     for p in rc.polys:
         x = O.uniform_rns(seed, p * bench.L, moduli, bench.N)
-        for _ in range(2):
+        for k in range(2):
             x = full.polymul_roundtrip(x, plain, threads=8).reshape(x.shape)
+            if k == 0:
+                rows1[p] = x.reshape(bench.L, bench.N).copy()
         rows[p] = x.reshape(bench.L, bench.N)
 
     def read(row):
         return rows[row // bench.L][row % bench.L]
 
     assert rc.check("two round trips", 2, read)
+    # a later leg may have run fewer round trips on its own copy of the batch
+    assert rc.check("one round trip", 1, lambda row: rows1[row // bench.L][row % bench.L])
+    assert rc.check("two round trips again", 2, read)
     assert rc.summary()["verified"]
-    # rows one limb off do not pass
+    # rows one limb off do not pass, nor rows one round trip off
     assert not rc.check("rows one limb off", 2, lambda row: rows[row // bench.L][(row + 1) % bench.L])
+    assert not rc.check("rows one round trip off", 1, read)
     assert not rc.summary()["verified"]
