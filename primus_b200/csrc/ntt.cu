@@ -404,6 +404,13 @@ static int check_table_data(const pg_ntt_table* t, const void* d, size_t polys) 
     return PG_OK;
 }
 
+#ifndef PG_PIPE_STREAMS
+#define PG_PIPE_STREAMS 3
+#endif
+#ifndef PG_PIPE_CHUNK_MB
+#define PG_PIPE_CHUNK_MB 64
+#endif
+
 // Host slices through a copy / compute pipeline: chunks of whole polys are
 // copied in on one of kPipeStreams streams, transformed there and copied back,
 // so that the two copy engines (host->device and device->host) and the SMs work
@@ -415,8 +422,8 @@ static int host_pipeline(const pg_ntt_table* t, uint64_t* h, size_t polys, int l
     int rc = check_table_data(t, h, polys);
     if (rc) return rc;
     if (polys == 0) return PG_OK;
-    constexpr int kPipeStreams = 3;
-    constexpr size_t kChunkBytes = 64ull << 20;
+    constexpr int kPipeStreams = PG_PIPE_STREAMS;
+    constexpr size_t kChunkBytes = (size_t)PG_PIPE_CHUNK_MB << 20;
     const size_t poly_words = (size_t)t->L * t->n;
     const size_t chunk = std::max<size_t>(1, kChunkBytes / (poly_words * sizeof(uint64_t)));
     const size_t nchunks = (polys + chunk - 1) / chunk;
