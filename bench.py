@@ -172,6 +172,22 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def host_description():
+    """The host the CPU legs ran on: CPU model, usable threads, AVX-512 IFMA."""
+    model, flags = "unknown", ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = line
+    except OSError:
+        pass
+    return {"cpu_model": model, "threads": cpu_threads(), "nproc": os.cpu_count(),
+            "avx512ifma": " avx512ifma" in flags}
+
+
 def cpu_reference(moduli, seconds_target=12.0, threads=None, path=None):
     """Time the reference's CPU path for this workload on the host cores over a bounded
     sample; returns (NTT/s, sample text, threads).  The path is the one the reference
@@ -208,7 +224,8 @@ def cpu_reference(moduli, seconds_target=12.0, threads=None, path=None):
         dt = time.perf_counter() - t0
         if dt >= seconds_target or reps >= 1000:
             break
-    return 2 * polys * reps / dt, f"{label}, OpenMP over rows; {polys} of {POLYS} polys (24 limbs, N=2^16) round " \
+    par = f"OpenMP over rows on {threads} threads" if threads > 1 else "one thread"
+    return 2 * polys * reps / dt, f"{label}, {par}; {polys} of {POLYS} polys (24 limbs, N=2^16) round " \
                                   f"trip x {reps}, {dt:.2f} s", threads
 
 
@@ -474,6 +491,9 @@ def run_gpu(args):
             if O.hexl_available():  # the scalar restatement beside it, on a short sample
                 sv, ssample, _ = cpu_reference(moduli, seconds_target=3.0, threads=thr, path="scalar")
                 cpu["scalar_port"] = {"value": sv, "sample": ssample}
+            sv1, ssample1, _ = cpu_reference(moduli, seconds_target=2.0, threads=1, path="scalar")
+            cpu["scalar_port_1_thread"] = {"value": sv1, "sample": ssample1}
+            cpu["host"] = host_description()
         workloads = None
         if world == 1 and not args.no_extra:
             workloads = {"polymul_n1024": bench_polymul_1024(P, stream),
