@@ -517,7 +517,9 @@ int pg_key_switch_hybrid(const pg_hybrid_ks *ks, uint32_t k_in, uint32_t k_out, 
  * into a CUDA graph and later runs of the same shape replay it. */
 typedef struct pg_polymul_job {
     uint64_t *d_a;          /* [moduli_count][N], result */
-    uint64_t *d_b;          /* [moduli_count][N], left in the NTT domain */
+    uint64_t *d_b;          /* [moduli_count][N], left in the NTT domain; both are transformed
+                               in place, so no buffer may overlap another of the same run
+                               (overlapping a and b of one job are refused) */
     uint32_t log_n;
     uint32_t moduli_count;
 } pg_polymul_job;

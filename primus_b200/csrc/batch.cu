@@ -208,6 +208,13 @@ int pg_polymul_batch_run(pg_polymul_batch* b, const pg_polymul_job* jobs, size_t
         if (jb.moduli_count == 0 || jb.moduli_count > b->tables[jb.log_n]->L)
             return set_error(PG_ERR_INVALID_ARGUMENT, "job moduli_count exceeds its table");
         if (!jb.d_a || !jb.d_b) return set_error(PG_ERR_INVALID_ARGUMENT, "job buffer is NULL");
+        {
+            // a and b are transformed in place: the two rows of a job must not overlap
+            const uintptr_t a0 = (uintptr_t)jb.d_a, b0 = (uintptr_t)jb.d_b;
+            const uintptr_t bytes = ((uintptr_t)jb.moduli_count << jb.log_n) * sizeof(uint64_t);
+            if (a0 < b0 + bytes && b0 < a0 + bytes)
+                return set_error(PG_ERR_INVALID_ARGUMENT, "job buffers a and b overlap (both are transformed in place)");
+        }
         rows[jb.log_n] += jb.moduli_count;
         maxL[jb.log_n] = std::max(maxL[jb.log_n], jb.moduli_count);
     }

@@ -462,6 +462,10 @@ int pg_server_submit(pg_server* srv, const pg_request* req, uint64_t* ticket) {
             if (t->log_n == req->log_n && req->moduli_count >= 1 && req->moduli_count <= t->L) ok = true;
         if (!ok || !req->d_a || !req->d_b)
             return set_error(PG_ERR_INVALID_ARGUMENT, "polymul request: no table for this degree / limb count");
+        const uintptr_t a0 = (uintptr_t)req->d_a, b0 = (uintptr_t)req->d_b;
+        const uintptr_t bytes = ((uintptr_t)req->moduli_count << req->log_n) * sizeof(uint64_t);
+        if (a0 < b0 + bytes && b0 < a0 + bytes)
+            return set_error(PG_ERR_INVALID_ARGUMENT, "polymul request: a and b overlap (both are transformed in place)");
     } else if (req->kind == PG_REQ_EXT_PRODUCT || req->kind == PG_REQ_KEY_SWITCH) {
         if (req->key >= srv->keys.size() || srv->keys[req->key].kind != req->kind || !req->d_in || !req->d_out)
             return set_error(PG_ERR_INVALID_ARGUMENT, "request names an unknown key or NULL buffers");

@@ -89,3 +89,11 @@ def test_rejects_bad_jobs(gpu):
         batch.run([(d, d, 11, 1)])   # no table for N = 2^11
     with pytest.raises(gpu.PrimusGpuError):
         batch.run([(d, d, 10, 3)])   # more limbs than the table
+    with pytest.raises(gpu.PrimusGpuError):
+        batch.run([(d, d, 10, 1)])   # a and b are the same row (both are transformed in place)
+
+    class View:  # a device pointer into d
+        def __init__(self, off):
+            self.ptr = d.ptr + 8 * off
+    with pytest.raises(gpu.PrimusGpuError):
+        batch.run([(View(0), View(1000), 10, 2)])  # b starts inside a's two rows

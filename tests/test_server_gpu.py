@@ -156,7 +156,8 @@ def test_malformed_requests_refused(gpu, env):
     bad = [P.ext_product_request(99, d, d),                      # unknown key
            P.key_switch_request(xid, d, d),                      # key of another kind
            P.polymul_request(d, d, 11, 1),                       # no table for N = 2^11
-           P.polymul_request(d, d, 10, 5)]                       # more limbs than the table
+           P.polymul_request(d, d, 10, 5),                       # more limbs than the table
+           P.polymul_request(d, d, 10, 1)]                       # a and b the same row
     for r in bad:
         st, _ = srv.try_submit(r)
         assert st == nat.PG_ERR_INVALID_ARGUMENT
