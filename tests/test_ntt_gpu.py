@@ -144,11 +144,11 @@ def test_host_slice_dropin_lazy(gpu):
 
 
 def test_host_slices_pipelined(gpu):
-    # 5 polys of 24 limbs at N = 2^16 (25 MB each): three chunks on the three
-    # pipeline streams, in pinned and in pageable host memory
+    # 12 polys of 24 limbs at N = 2^16 (12.6 MB each): 64 MB chunks of 5, 5 and 2
+    # polys on the three pipeline streams, in pinned and in pageable host memory
     import ctypes as C
     from primus_b200 import _native as nat
-    log_n, L, polys = 16, 24, 5
+    log_n, L, polys = 16, 24, 12
     n = 1 << log_n
     moduli = O.ntt_primes(1 << 50, 2 * n, L)
     tab = gpu.DcrtTable(log_n, moduli)
