@@ -13,8 +13,11 @@ flush is needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Prints one JSON line.  `--impl reference` times the CPU restatement of the
-reference's own algorithm (the oracle port; the Rust reference cannot be built
-here) on the host's cores over a bounded sample of the same workload.
+reference's own algorithm (the oracle port of its Rust code) on the host's
+cores over a bounded sample of the same workload.  The line also carries the
+end-to-end rate through the C ABI with host buffers (beside the host link's
+own rate), the roofline of the fused kernel, the CPU baseline and the check of
+the timed output against the oracle.
 """
 from __future__ import annotations
 
