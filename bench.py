@@ -428,7 +428,7 @@ def run_gpu(args):
     e2e_ms = dist_max(dist, e0.elapsed_ms(e1) / e2e_steps, local)
     check.check("end to end through the host-slice call", rounds + 2 + e2e_steps,
                 lambda row: host[row * N:(row + 1) * N].copy())
-    # the host link of this box: the step's H2D and D2H bytes as two concurrent copies
+    # the host link of the machine: the step's H2D and D2H bytes as two concurrent copies
     # on two streams with no kernels (one cudaMemcpyAsync each); the end-to-end leg
     # cannot run faster than this
     hp2 = C.c_void_p()
@@ -520,7 +520,7 @@ def run_gpu(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "ms_per_step": e2e_ms, "path": "pg_dcrt_polymul_ntt_plain_host (pinned host slice; chunked H2D / fused launch / D2H on 3 streams)",
                     "host_link_ms_per_step": link_ms, "frac_of_host_link": link_ms / e2e_ms,
-                    "host_link_note": "the same H2D and D2H bytes as two concurrent copies, no kernels (this box)"},
+                    "host_link_note": "the same H2D and D2H bytes as two concurrent copies, no kernels (this machine)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": load_traffic(), "peak_source": peak_kind,

@@ -5,9 +5,10 @@ check in __graft_entry__.py and bench.py's CPU-baseline / reference arm import
 it.  The product package (primus_b200) never imports it.
 
 The oracle restates the reference's Rust functions in C (each C function
-cites the crate file:line it follows).  The reference itself cannot be built
-in this image (no Rust toolchain), so the restatement is pinned by the
-reference's own known-answer and property tests (tests/test_oracle_pins.py).
+cites the crate file:line it follows).  The reference itself is a Rust
+workspace that is not compiled or run next to this package, so the restatement
+is pinned by the reference's own known-answer and property tests
+(tests/test_oracle_pins.py).
 """
 from __future__ import annotations
 

@@ -7,7 +7,7 @@
  *
  * Every function restates one reference function (Rust crate path:line in the
  * comment above its definition in primus_oracle.c).  The reference is a Rust
- * workspace and cannot be compiled in this image (no cargo/rustc), so the
+ * workspace that is not compiled or run next to this library, so the
  * restatement is pinned by the reference's own known-answer tests and
  * property tests (tests/test_oracle_pins.py) rather than by running it.
  *

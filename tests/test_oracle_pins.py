@@ -1,6 +1,6 @@
 """Pins the CPU oracle to the reference before parity tests rely on it.
 
-The reference (Rust) cannot be built in this image, so the oracle is pinned by
+The reference (a Rust workspace) is not compiled or run alongside these tests, so the oracle is pinned by
 (a) the golden fixtures in tests/golden/ -- pure-Python big-integer values of
 the definitions the reference encodes -- and (b) ports of the reference's own
 known-answer and property tests, with fixed seeds:
